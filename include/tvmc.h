@@ -1,0 +1,183 @@
+/*
+ * tvmc -- B200 (sm_100a) table-commitment library, C ABI.
+ *
+ * The table-commitment path of the Triton VM prover: per-column low-degree
+ * extension (LDE) over Goldilocks p = 2^64 - 2^32 + 1, the Tip5 hash of every
+ * LDE row, and the Tip5 Merkle tree over the row digests.  Every result is
+ * bit-identical to the reference prover's CPU path (canonical field elements).
+ *
+ * Conventions
+ *   - Field elements are uint64_t.  Inputs >= p are accepted and read as their
+ *     residue mod p (the reference's BFieldElement(uint64_t) constructor does
+ *     the same); every output is canonical (< p).
+ *   - A digest is 5 consecutive uint64_t.
+ *   - "Column-major" table: element (row r, column c) at ptr[c*len + r].
+ *     "Row-major": ptr[r*width + c].  An XFieldElement column contributes three
+ *     consecutive base columns (c0, c1, c2), the order in which the reference
+ *     flattens aux rows for hashing (src/table/table_commitment.cpp:65-77).
+ *   - Functions named *_gpu take DEVICE pointers, are stream-ordered and
+ *     return after enqueueing work; `stream` is a cudaStream_t (NULL = the
+ *     legacy default stream).  Functions named *_host take HOST pointers and
+ *     return when the result is in host memory.
+ *   - Every function returns a tvmc status; tvmc_last_error() describes the
+ *     most recent failure on the calling thread.
+ *   - Thread safety: the library is safe to call from several threads; one
+ *     commitment handle must not be used from two threads at once.
+ *   - The first call on a device builds twiddle tables with synchronous copies;
+ *     make one call before capturing work into a CUDA graph.
+ *
+ * Reference interfaces replaced are cited per entry point (paths inside the
+ * reference project).
+ */
+#ifndef TVMC_H
+#define TVMC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+#define TVMC_OK 0
+#define TVMC_ERR_INVALID 1     /* size not a power of two, zero width, bad flag ... */
+#define TVMC_ERR_RANGE 2       /* leaf / row index out of range */
+#define TVMC_ERR_NOMEM 3       /* device allocation or admission failure */
+#define TVMC_ERR_CUDA 4        /* CUDA runtime error (see tvmc_last_error) */
+#define TVMC_ERR_TIMEOUT 5     /* a bounded device wait expired */
+#define TVMC_ERR_UNSUPPORTED 6 /* size beyond what this build supports */
+
+/* Largest supported sizes (log2). */
+#define TVMC_MAX_LOG_NTT 24       /* plain NTT length */
+#define TVMC_MAX_LOG_LDE_TRACE 22 /* LDE trace length; LDE length up to 2^26 */
+
+const char* tvmc_last_error(void);
+const char* tvmc_status_string(int status);
+int tvmc_version(void);
+/* Number of CUDA devices visible (0 when no GPU); never fails. */
+int tvmc_device_count(void);
+
+/* ---- NTT (include/gpu/kernels/ntt_kernel.cuh:88-106, src/ntt/ntt.cpp:59-86) ---- */
+
+/* In-place forward NTT of num_cols column-major columns of length n
+ * (d_data[col*n + row]); natural order in and out; w = 7^((p-1)/n).
+ * Replaces triton_vm::gpu::kernels::ntt_forward_batched_gpu. */
+int tvmc_ntt_forward_batched_gpu(uint64_t* d_data, size_t n, size_t num_cols, void* stream);
+/* In-place inverse NTT (w^-1, scaled by n^-1).
+ * Replaces triton_vm::gpu::kernels::ntt_inverse_batched_gpu. */
+int tvmc_ntt_inverse_batched_gpu(uint64_t* d_data, size_t n, size_t num_cols, void* stream);
+/* Host-buffer form of the two above (NTT::forward / NTT::inverse on each column). */
+int tvmc_ntt_host(uint64_t* data, size_t n, size_t num_cols, int inverse);
+
+/* ---- LDE (include/gpu/kernels/lde_kernel.cuh lde_batch_gpu; src/ntt/ntt.cpp:121-131) ---- */
+
+/* Low-degree extension of num_columns column-major columns: interpolate each
+ * column on the size-trace_len subgroup, then evaluate on
+ * extended_offset * <w_extended_len>.  trace_offset is ignored, as in the
+ * reference's LDE::extend_column and lde_column_gpu.  extended_len must be
+ * trace_len * 2^k with 0 <= k <= 4.  Replaces lde_batch_gpu. */
+int tvmc_lde_batch_gpu(const uint64_t* d_traces, size_t num_columns, size_t trace_len, uint64_t* d_extended,
+                       size_t extended_len, uint64_t trace_offset, uint64_t extended_offset, void* stream);
+/* Host-buffer form (LDE::extend_table on column-major data). */
+int tvmc_lde_host(const uint64_t* traces, size_t num_columns, size_t trace_len, uint64_t* extended,
+                  size_t extended_len, uint64_t extended_offset);
+
+/* ---- Tip5 (include/gpu/kernels/row_hash_kernel.cuh:26-49, src/hash/tip5.cpp) ---- */
+
+/* Tip5::hash_varlen of every row of a column-major table (d_table[col*num_rows + row]).
+ * Replaces hash_bfield_rows_gpu. */
+int tvmc_hash_bfield_rows_gpu(const uint64_t* d_table, size_t num_rows, size_t num_cols, uint64_t* d_digests,
+                              void* stream);
+/* Same for an XFieldElement table stored as (xfe_col*3 + component)*num_rows + row.
+ * Replaces hash_xfield_rows_gpu. */
+int tvmc_hash_xfield_rows_gpu(const uint64_t* d_table, size_t num_rows, size_t num_xfe_cols,
+                              uint64_t* d_digests, void* stream);
+/* Tip5::hash_varlen of num_rows host rows of row_len elements each (row-major). */
+int tvmc_hash_varlen_host(const uint64_t* rows, size_t num_rows, size_t row_len, uint64_t* digests);
+/* Tip5::hash_pair on count pairs (Backend::hash_pairs, include/backend/backend.hpp:106-120). */
+int tvmc_hash_pairs_gpu(const uint64_t* d_left, const uint64_t* d_right, uint64_t* d_out, size_t count,
+                        void* stream);
+int tvmc_hash_pairs_host(const uint64_t* left, const uint64_t* right, uint64_t* out, size_t count);
+/* Tip5 permutation of num_states 16-word states in place
+ * (Backend::tip5_permutation_batch, include/backend/backend.hpp:99-104). */
+int tvmc_tip5_permutation_batch_gpu(uint64_t* d_states, size_t num_states, void* stream);
+int tvmc_tip5_permutation_batch_host(uint64_t* states, size_t num_states);
+
+/* ---- Merkle (include/gpu/kernels/merkle_kernel.cuh:26-50, src/merkle/merkle_tree.cpp) ---- */
+
+/* Full tree in the reference GPU layout: d_tree holds 2n-1 digests
+ * [leaves | level 1 | ... | root], root at index 2n-2.  Replaces merkle_tree_gpu. */
+int tvmc_merkle_tree_gpu(const uint64_t* d_leaves, uint64_t* d_tree, size_t num_leaves, void* stream);
+/* Root only (5 words to device memory).  Replaces merkle_root_gpu. */
+int tvmc_merkle_root_gpu(const uint64_t* d_leaves, uint64_t* d_root, size_t num_leaves, void* stream);
+/* Heap layout, as the reference's CPU MerkleTree: nodes holds 2n digests,
+ * node 1 is the root, leaves at [n, 2n), node 0 is written as zeros. */
+int tvmc_merkle_tree_heap_host(const uint64_t* leaves, size_t num_leaves, uint64_t* nodes);
+
+/* ---- table commitment (the whole path; src/gpu/gpu_stark.cu:2132-2617 step 2/3,
+ *      src/stark.cpp:1163-1196, LDETable::compute_lde_and_merkle src/lde/lde_table.cpp:86-101) ---- */
+
+typedef struct tvmc_commitment tvmc_commitment;
+
+#define TVMC_TRACE_DEVICE 0x1u    /* trace is a device pointer (else host) */
+#define TVMC_TRACE_ROW_MAJOR 0x2u /* trace is row-major [trace_len][width] (else column-major) */
+#define TVMC_DISCARD_LDE 0x4u     /* free the LDE after hashing; keep only the tree */
+#define TVMC_SYNC 0x8u            /* return only when the commitment is complete */
+#define TVMC_PROFILE 0x10u        /* record CUDA events around the upload, LDE and hash/tree phases */
+
+/* Commit to one table: LDE of every column onto offset * <w_{trace_len*expansion}>
+ * (expansion a power of two <= 16), Tip5 hash_varlen of every LDE row, Merkle
+ * tree over the row digests.  The LDE (column-major, len trace_len*expansion)
+ * and the heap-layout tree stay in device memory, owned by *out, until
+ * tvmc_commitment_free.  Work is enqueued on `stream`. */
+int tvmc_commit(const uint64_t* trace, size_t trace_len, size_t width, uint32_t expansion, uint64_t offset,
+                uint32_t flags, void* stream, tvmc_commitment** out);
+/* Wait for the commitment and copy its root (5 words) to host memory. */
+int tvmc_commitment_root(tvmc_commitment* c, uint64_t* root);
+int tvmc_commitment_sync(tvmc_commitment* c);
+/* Sizes: LDE length (= number of leaves) and width. */
+int tvmc_commitment_shape(const tvmc_commitment* c, size_t* lde_len, size_t* width);
+/* Device pointers: column-major LDE (NULL after TVMC_DISCARD_LDE) and heap tree. */
+int tvmc_commitment_device_lde(const tvmc_commitment* c, const uint64_t** d_lde);
+int tvmc_commitment_device_tree(const tvmc_commitment* c, const uint64_t** d_nodes);
+/* Authentication paths (MerkleTree::authentication_path, src/merkle/merkle_tree.cpp:93-113):
+ * out holds count * log2(lde_len) digests, path of leaf_idx[q] first-sibling first. */
+int tvmc_commitment_auth_paths(tvmc_commitment* c, const size_t* leaf_idx, size_t count, uint64_t* out);
+/* Batched authentication structure (MerkleTree::authentication_structure,
+ * src/merkle/merkle_tree.cpp:115-226): digests of the needed-but-not-computable
+ * nodes in descending heap-index order.  Writes at most max_digests digests and
+ * sets *num_digests to the full count. */
+int tvmc_commitment_auth_structure(tvmc_commitment* c, const size_t* leaf_idx, size_t count, uint64_t* out,
+                                   size_t max_digests, size_t* num_digests);
+/* Heap indices of the authentication structure for leaf_idx over a tree of
+ * num_leaves leaves, descending (MerkleTree::authentication_structure_node_indices,
+ * src/merkle/merkle_tree.cpp:228-262).  Host-only; no device work. */
+int tvmc_auth_structure_indices(size_t num_leaves, const size_t* leaf_idx, size_t count, uint64_t* out,
+                                size_t max_out, size_t* num_out);
+/* Rows of the LDE, row-major: out[q*width + col] = LDE[rows[q]][col]. */
+int tvmc_commitment_read_rows(tvmc_commitment* c, const size_t* rows, size_t count, uint64_t* out);
+/* Columns [col0, col0 + ncols) of the LDE to host memory, column-major. */
+int tvmc_commitment_read_columns(tvmc_commitment* c, size_t col0, size_t ncols, uint64_t* out);
+/* The whole LDE to host memory, column-major (or row-major with row_major != 0). */
+int tvmc_commitment_read_lde(tvmc_commitment* c, uint64_t* out, int row_major);
+/* All leaf digests (lde_len x 5) / all heap nodes (2*lde_len x 5) to host memory. */
+int tvmc_commitment_read_leaves(tvmc_commitment* c, uint64_t* out);
+int tvmc_commitment_read_nodes(tvmc_commitment* c, uint64_t* out);
+int tvmc_commitment_free(tvmc_commitment* c);
+/* For a TVMC_PROFILE commitment: device milliseconds of [upload (or transpose),
+ * LDE, row hash + Merkle tree]; with a pipelined host upload the upload is
+ * counted inside the LDE phase. */
+int tvmc_commitment_phase_ms(tvmc_commitment* c, float* ms3);
+/* Total kernels launched by this library so far (all threads and devices). */
+unsigned long long tvmc_launch_count(void);
+/* Measured 32-bit integer instruction issue rate of the current device
+ * (thread-instructions per second, an even IMAD/ALU mix); the denominator of
+ * the Tip5 roofline.  Synchronizes `stream`; returns < 0 on failure.
+ * No reference counterpart (measurement utility). */
+double tvmc_int_peak_probe(void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TVMC_H */

@@ -1,0 +1,785 @@
+// C ABI of the table-commitment library (declared in include/tvmc.h).
+//
+// Host side: argument checking with the reference's error semantics, the
+// per-device twiddle-table cache, stream-ordered scratch (cudaMallocAsync from
+// the device's default pool), and the commitment handle that keeps the LDE and
+// the Merkle tree resident for later openings.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "internal.cuh"
+#include "tvmc.h"
+
+using namespace tvmc;
+
+namespace {
+std::atomic<unsigned long long> g_launches{0};
+}
+
+void tvmc::count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* where) {
+    if (e == cudaErrorMemoryAllocation) return fail(TVMC_ERR_NOMEM, "%s: %s", where, cudaGetErrorString(e));
+    return fail(TVMC_ERR_CUDA, "%s: %s", where, cudaGetErrorString(e));
+}
+
+#define CK(expr)                                            \
+    do {                                                    \
+        cudaError_t e_ = (expr);                            \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #expr); \
+    } while (0)
+
+bool is_pow2(size_t n) { return n != 0 && (n & (n - 1)) == 0; }
+int log2u(size_t n) {
+    int k = 0;
+    while ((size_t(1) << k) < n) k++;
+    return k;
+}
+
+// ---- host Goldilocks (table construction only) ----
+constexpr uint64_t P = 0xFFFFFFFF00000001ull;
+uint64_t hmul(uint64_t a, uint64_t b) { return (uint64_t)(((unsigned __int128)a * b) % P); }
+uint64_t hpow(uint64_t b, uint64_t e) {
+    uint64_t r = 1;
+    b %= P;
+    while (e) {
+        if (e & 1) r = hmul(r, b);
+        b = hmul(b, b);
+        e >>= 1;
+    }
+    return r;
+}
+uint64_t hinv(uint64_t a) { return hpow(a, P - 2); }
+uint64_t root_of_unity(int k) { return hpow(7, (P - 1) >> k); }
+
+// ---- per-device table cache ----
+struct DevTables {
+    uint64_t* tw12_f = nullptr;
+    uint64_t* tw12_i = nullptr;
+    std::map<int, std::pair<uint64_t*, uint64_t*>> wn_f, wn_i;                  // logn -> (lo, hi)
+    std::map<std::tuple<int, int, uint64_t>, std::pair<uint64_t*, uint64_t*>> sc;  // (logn, le, offset)
+    bool pool_set = false;
+};
+std::mutex g_mu;
+std::map<int, DevTables> g_dev;
+
+cudaError_t upload(const std::vector<uint64_t>& h, uint64_t** d) {
+    cudaError_t e = cudaMalloc(d, h.size() * 8);
+    if (e != cudaSuccess) return e;
+    return cudaMemcpy(*d, h.data(), h.size() * 8, cudaMemcpyHostToDevice);
+}
+
+int current_device(int* dev) {
+    CK(cudaGetDevice(dev));
+    return TVMC_OK;
+}
+
+// Builds (once per device) the tables needed for size 2^logn and, if le >= 0,
+// the LDE coset scales for expansion 2^le and `offset`.
+int get_plan(int logn, int le, uint64_t offset, LdePlan* pl) {
+    int dev;
+    int rc = current_device(&dev);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(g_mu);
+    DevTables& T = g_dev[dev];
+    if (!T.pool_set) {
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+            uint64_t thr = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+        }
+        T.pool_set = true;
+    }
+    if (!T.tw12_f) {
+        std::vector<uint64_t> f(2048), i(2048);
+        uint64_t w = root_of_unity(12), wi = hinv(w), x = 1, y = 1;
+        for (int m = 0; m < 2048; m++) {
+            f[m] = x;
+            i[m] = y;
+            x = hmul(x, w);
+            y = hmul(y, wi);
+        }
+        CK(upload(f, &T.tw12_f));
+        CK(upload(i, &T.tw12_i));
+    }
+    auto make_wn = [&](bool inv, std::pair<uint64_t*, uint64_t*>* out) -> int {
+        uint64_t w = root_of_unity(logn);
+        if (inv) w = hinv(w);
+        size_t hi_len = logn > 12 ? (size_t(1) << (logn - 12)) : 1;
+        std::vector<uint64_t> lo(4096), hi(hi_len);
+        uint64_t x = 1;
+        for (int e = 0; e < 4096; e++) { lo[e] = x; x = hmul(x, w); }
+        uint64_t w4096 = hpow(w, 4096);
+        x = 1;
+        for (size_t j = 0; j < hi_len; j++) { hi[j] = x; x = hmul(x, w4096); }
+        CK(upload(lo, &out->first));
+        CK(upload(hi, &out->second));
+        return TVMC_OK;
+    };
+    if (!T.wn_f.count(logn)) {
+        std::pair<uint64_t*, uint64_t*> a{}, b{};
+        if ((rc = make_wn(false, &a))) return rc;
+        if ((rc = make_wn(true, &b))) return rc;
+        T.wn_f[logn] = a;
+        T.wn_i[logn] = b;
+    }
+    pl->logn = logn;
+    pl->log_exp = le < 0 ? 0 : le;
+    pl->offset = offset;
+    pl->tw12_f = T.tw12_f;
+    pl->tw12_i = T.tw12_i;
+    pl->wn_f_lo = T.wn_f[logn].first;
+    pl->wn_f_hi = T.wn_f[logn].second;
+    pl->wn_i_lo = T.wn_i[logn].first;
+    pl->wn_i_hi = T.wn_i[logn].second;
+    pl->sc_lo = pl->sc_hi = nullptr;
+    if (le >= 0) {
+        auto key = std::make_tuple(logn, le, offset % P);
+        if (!T.sc.count(key)) {
+            int E = 1 << le;
+            size_t N = size_t(1) << logn;
+            size_t hi_len = logn > 12 ? (size_t(1) << (logn - 12)) : 1;
+            uint64_t wEN = root_of_unity(logn + le);
+            uint64_t ninv = hinv(N % P);
+            std::vector<uint64_t> lo(4096 * (size_t)E), hi(hi_len * (size_t)E);
+            for (int c = 0; c < E; c++) {
+                uint64_t s = hmul(offset % P, hpow(wEN, (uint64_t)c));
+                uint64_t x = 1;
+                for (int e = 0; e < 4096; e++) { lo[4096 * c + e] = x; x = hmul(x, s); }
+                uint64_t s4096 = hpow(s, 4096);
+                x = ninv;
+                for (size_t j = 0; j < hi_len; j++) { hi[hi_len * c + j] = x; x = hmul(x, s4096); }
+            }
+            std::pair<uint64_t*, uint64_t*> pr{};
+            CK(upload(lo, &pr.first));
+            CK(upload(hi, &pr.second));
+            T.sc[key] = pr;
+        }
+        pl->sc_lo = T.sc[key].first;
+        pl->sc_hi = T.sc[key].second;
+    }
+    return TVMC_OK;
+}
+
+cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// Column chunk so that LDE scratch stays under ~2 GiB.
+size_t lde_chunk_cols(int logn, int le, size_t width) {
+    size_t per = lde_scratch_words(logn, le, 1) * 8;
+    if (per == 0) return width ? width : 1;
+    size_t lim = (size_t(2) << 30) / per;
+    if (lim < 1) lim = 1;
+    return std::min(width ? width : size_t(1), lim);
+}
+
+int run_lde(const LdePlan& pl, const uint64_t* d_tr, uint64_t tld, uint64_t* d_out, uint64_t old, size_t width,
+            cudaStream_t st) {
+    size_t chunk = lde_chunk_cols(pl.logn, pl.log_exp, width);
+    size_t sw = lde_scratch_words(pl.logn, pl.log_exp, chunk);
+    uint64_t* scratch = nullptr;
+    if (sw) CK(cudaMallocAsync((void**)&scratch, sw * 8, st));
+    for (size_t c0 = 0; c0 < width; c0 += chunk) {
+        size_t nc = std::min(chunk, width - c0);
+        cudaError_t e = launch_lde(pl, d_tr + c0 * tld, tld, d_out + c0 * old, old, nc, scratch, st);
+        if (e != cudaSuccess) {
+            if (scratch) cudaFreeAsync(scratch, st);
+            return cuda_fail(e, "launch_lde");
+        }
+    }
+    if (scratch) CK(cudaFreeAsync(scratch, st));
+    return TVMC_OK;
+}
+
+// Per-device non-blocking stream for host->device uploads.
+std::map<int, cudaStream_t> g_copy_streams;
+
+int copy_stream(cudaStream_t* out) {
+    int dev;
+    int rc = current_device(&dev);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto it = g_copy_streams.find(dev);
+    if (it == g_copy_streams.end()) {
+        cudaStream_t s;
+        CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        it = g_copy_streams.emplace(dev, s).first;
+    }
+    *out = it->second;
+    return TVMC_OK;
+}
+
+// Host column-major trace -> device LDE.  Column chunks are staged through two
+// device buffers: the copy stream uploads chunk k+1 while `st` runs the LDE of
+// chunk k.  Returns after enqueueing; `st` is ordered after every copy.
+int upload_lde_pipelined(const LdePlan& pl, const uint64_t* h_trace, size_t n, size_t width, uint64_t* d_out,
+                         size_t L, cudaStream_t st) {
+    cudaStream_t cs;
+    int rc = copy_stream(&cs);
+    if (rc) return rc;
+    size_t chunk = lde_chunk_cols(pl.logn, pl.log_exp, width);
+    // keep staging chunks near 256 MB so the first upload is short
+    size_t stage_cols = std::max<size_t>(1, (size_t(256) << 20) / (n * 8));
+    chunk = std::min(chunk, stage_cols);
+    const size_t nchunks = (width + chunk - 1) / chunk;
+    const size_t sw = lde_scratch_words(pl.logn, pl.log_exp, chunk);
+    uint64_t *scratch = nullptr, *stage[2] = {nullptr, nullptr};
+    cudaEvent_t ready[2] = {nullptr, nullptr}, freed[2] = {nullptr, nullptr};
+    cudaError_t e = cudaSuccess;
+    if (sw) e = cudaMallocAsync((void**)&scratch, sw * 8, st);
+    for (int b = 0; b < 2 && e == cudaSuccess; b++) {
+        e = cudaMallocAsync((void**)&stage[b], chunk * n * 8, st);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ready[b], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&freed[b], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventRecord(freed[b], st);  // allocations are ordered on st
+    }
+    for (size_t k = 0; k < nchunks && e == cudaSuccess; k++) {
+        const int b = (int)(k & 1);
+        const size_t c0 = k * chunk, nc = std::min(chunk, width - c0);
+        e = cudaStreamWaitEvent(cs, freed[b], 0);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(stage[b], h_trace + c0 * n, nc * n * 8, cudaMemcpyHostToDevice, cs);
+        if (e == cudaSuccess) e = cudaEventRecord(ready[b], cs);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(st, ready[b], 0);
+        if (e == cudaSuccess) e = launch_lde(pl, stage[b], n, d_out + c0 * L, L, nc, scratch, st);
+        if (e == cudaSuccess) e = cudaEventRecord(freed[b], st);
+    }
+    for (int b = 0; b < 2; b++) {
+        if (stage[b]) cudaFreeAsync(stage[b], st);
+        if (ready[b]) cudaEventDestroy(ready[b]);  // destruction is deferred until the event completes
+        if (freed[b]) cudaEventDestroy(freed[b]);
+    }
+    if (scratch) cudaFreeAsync(scratch, st);
+    if (e != cudaSuccess) return cuda_fail(e, "pipelined upload/LDE");
+    return TVMC_OK;
+}
+
+int check_lde_sizes(size_t trace_len, size_t extended_len, int* logn, int* le) {
+    if (!is_pow2(trace_len)) return fail(TVMC_ERR_INVALID, "trace length %zu is not a power of 2", trace_len);
+    if (!is_pow2(extended_len) || extended_len < trace_len)
+        return fail(TVMC_ERR_INVALID, "extended length %zu is not a power of 2 >= trace length", extended_len);
+    *logn = log2u(trace_len);
+    *le = log2u(extended_len) - *logn;
+    if (*logn > MAX_LOG_LDE_TRACE)
+        return fail(TVMC_ERR_UNSUPPORTED, "LDE trace length 2^%d exceeds 2^%d", *logn, MAX_LOG_LDE_TRACE);
+    if (*le > 4) return fail(TVMC_ERR_UNSUPPORTED, "expansion factor 2^%d exceeds 16", *le);
+    return TVMC_OK;
+}
+
+int ntt_impl(uint64_t* d, size_t n, size_t cols, int inverse, cudaStream_t st) {
+    if (!is_pow2(n)) return fail(TVMC_ERR_INVALID, "NTT size must be a power of 2 (got %zu)", n);
+    int l = log2u(n);
+    if (l > MAX_LOG_NTT) return fail(TVMC_ERR_UNSUPPORTED, "NTT size 2^%d exceeds 2^%d", l, MAX_LOG_NTT);
+    if (cols == 0) return TVMC_OK;
+    LdePlan pl;
+    int rc = get_plan(l, -1, 0, &pl);
+    if (rc) return rc;
+    size_t sw = ntt_scratch_words(l, cols);
+    uint64_t* scratch = nullptr;
+    if (sw) CK(cudaMallocAsync((void**)&scratch, sw * 8, st));
+    cudaError_t e = launch_ntt(pl, inverse, d, n, cols, scratch, st);
+    if (scratch) cudaFreeAsync(scratch, st);
+    if (e != cudaSuccess) return cuda_fail(e, "launch_ntt");
+    return TVMC_OK;
+}
+
+// RAII device buffer for host-API calls.
+struct DBuf {
+    uint64_t* p = nullptr;
+    ~DBuf() {
+        if (p) cudaFree(p);
+    }
+    cudaError_t alloc(size_t words) { return cudaMalloc((void**)&p, words ? words * 8 : 8); }
+};
+
+// Needed-minus-computable node set of a batch of leaf paths, descending.
+int auth_structure_nodes(size_t n, const size_t* leaf_idx, size_t count, std::vector<uint64_t>* res) {
+    std::vector<uint64_t> path, need;
+    for (size_t q = 0; q < count; q++) {
+        if (leaf_idx[q] >= n) return fail(TVMC_ERR_RANGE, "Leaf index %zu out of range", leaf_idx[q]);
+        for (uint64_t i = n + leaf_idx[q]; i > 1; i >>= 1) {
+            path.push_back(i);
+            need.push_back(i ^ 1);
+        }
+    }
+    std::sort(path.begin(), path.end());
+    path.erase(std::unique(path.begin(), path.end()), path.end());
+    std::sort(need.begin(), need.end());
+    need.erase(std::unique(need.begin(), need.end()), need.end());
+    res->clear();
+    std::set_difference(need.begin(), need.end(), path.begin(), path.end(), std::back_inserter(*res));
+    std::reverse(res->begin(), res->end());
+    return TVMC_OK;
+}
+
+}  // namespace
+
+struct tvmc_commitment {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    size_t n = 0, width = 0, L = 0;
+    uint64_t* d_lde = nullptr;
+    uint64_t* d_nodes = nullptr;
+    cudaEvent_t done = nullptr;
+    // TVMC_PROFILE: events at start / after upload / after LDE / after hash+tree
+    cudaEvent_t prof[4] = {nullptr, nullptr, nullptr, nullptr};
+};
+
+extern "C" {
+
+const char* tvmc_last_error(void) { return g_err.c_str(); }
+
+const char* tvmc_status_string(int s) {
+    switch (s) {
+        case TVMC_OK: return "ok";
+        case TVMC_ERR_INVALID: return "invalid argument";
+        case TVMC_ERR_RANGE: return "index out of range";
+        case TVMC_ERR_NOMEM: return "out of device memory";
+        case TVMC_ERR_CUDA: return "CUDA error";
+        case TVMC_ERR_TIMEOUT: return "device wait timed out";
+        case TVMC_ERR_UNSUPPORTED: return "unsupported size";
+        default: return "unknown status";
+    }
+}
+
+int tvmc_version(void) { return 1; }
+
+unsigned long long tvmc_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
+int tvmc_device_count(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+// ---------------------------------------------------------------- NTT
+
+int tvmc_ntt_forward_batched_gpu(uint64_t* d_data, size_t n, size_t num_cols, void* stream) {
+    return ntt_impl(d_data, n, num_cols, 0, as_stream(stream));
+}
+int tvmc_ntt_inverse_batched_gpu(uint64_t* d_data, size_t n, size_t num_cols, void* stream) {
+    return ntt_impl(d_data, n, num_cols, 1, as_stream(stream));
+}
+
+int tvmc_ntt_host(uint64_t* data, size_t n, size_t num_cols, int inverse) {
+    if (!is_pow2(n)) return fail(TVMC_ERR_INVALID, "NTT size must be a power of 2 (got %zu)", n);
+    DBuf d;
+    CK(d.alloc(n * num_cols));
+    CK(cudaMemcpy(d.p, data, n * num_cols * 8, cudaMemcpyHostToDevice));
+    int rc = ntt_impl(d.p, n, num_cols, inverse, nullptr);
+    if (rc) return rc;
+    CK(cudaMemcpy(data, d.p, n * num_cols * 8, cudaMemcpyDeviceToHost));
+    return TVMC_OK;
+}
+
+// ---------------------------------------------------------------- LDE
+
+int tvmc_lde_batch_gpu(const uint64_t* d_traces, size_t num_columns, size_t trace_len, uint64_t* d_extended,
+                       size_t extended_len, uint64_t trace_offset, uint64_t extended_offset, void* stream) {
+    (void)trace_offset;
+    int logn, le;
+    int rc = check_lde_sizes(trace_len, extended_len, &logn, &le);
+    if (rc) return rc;
+    if (num_columns == 0) return TVMC_OK;
+    LdePlan pl;
+    if ((rc = get_plan(logn, le, extended_offset, &pl))) return rc;
+    return run_lde(pl, d_traces, trace_len, d_extended, extended_len, num_columns, as_stream(stream));
+}
+
+int tvmc_lde_host(const uint64_t* traces, size_t num_columns, size_t trace_len, uint64_t* extended,
+                  size_t extended_len, uint64_t extended_offset) {
+    int logn, le;
+    int rc = check_lde_sizes(trace_len, extended_len, &logn, &le);
+    if (rc) return rc;
+    if (num_columns == 0) return TVMC_OK;
+    DBuf a, b;
+    CK(a.alloc(trace_len * num_columns));
+    CK(b.alloc(extended_len * num_columns));
+    CK(cudaMemcpy(a.p, traces, trace_len * num_columns * 8, cudaMemcpyHostToDevice));
+    if ((rc = tvmc_lde_batch_gpu(a.p, num_columns, trace_len, b.p, extended_len, 1, extended_offset, nullptr)))
+        return rc;
+    CK(cudaMemcpy(extended, b.p, extended_len * num_columns * 8, cudaMemcpyDeviceToHost));
+    return TVMC_OK;
+}
+
+// ---------------------------------------------------------------- Tip5
+
+int tvmc_hash_bfield_rows_gpu(const uint64_t* d_table, size_t num_rows, size_t num_cols, uint64_t* d_digests,
+                              void* stream) {
+    CK(launch_hash_rows(d_table, 1, num_rows, num_rows, (uint32_t)num_cols, d_digests, nullptr, LAYOUT_HEAP,
+                        as_stream(stream)));
+    return TVMC_OK;
+}
+
+int tvmc_hash_xfield_rows_gpu(const uint64_t* d_table, size_t num_rows, size_t num_xfe_cols,
+                              uint64_t* d_digests, void* stream) {
+    return tvmc_hash_bfield_rows_gpu(d_table, num_rows, 3 * num_xfe_cols, d_digests, stream);
+}
+
+int tvmc_hash_varlen_host(const uint64_t* rows, size_t num_rows, size_t row_len, uint64_t* digests) {
+    if (num_rows == 0) return TVMC_OK;
+    DBuf a, b;
+    CK(a.alloc(num_rows * row_len));
+    CK(b.alloc(num_rows * 5));
+    if (row_len) CK(cudaMemcpy(a.p, rows, num_rows * row_len * 8, cudaMemcpyHostToDevice));
+    CK(launch_hash_rows(a.p, row_len, 1, num_rows, (uint32_t)row_len, b.p, nullptr, LAYOUT_HEAP, nullptr));
+    CK(cudaMemcpy(digests, b.p, num_rows * 40, cudaMemcpyDeviceToHost));
+    return TVMC_OK;
+}
+
+int tvmc_hash_pairs_gpu(const uint64_t* d_left, const uint64_t* d_right, uint64_t* d_out, size_t count,
+                        void* stream) {
+    CK(launch_hash_pairs(d_left, d_right, d_out, count, as_stream(stream)));
+    return TVMC_OK;
+}
+
+int tvmc_hash_pairs_host(const uint64_t* left, const uint64_t* right, uint64_t* out, size_t count) {
+    if (count == 0) return TVMC_OK;
+    DBuf a, b, c;
+    CK(a.alloc(5 * count));
+    CK(b.alloc(5 * count));
+    CK(c.alloc(5 * count));
+    CK(cudaMemcpy(a.p, left, 40 * count, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b.p, right, 40 * count, cudaMemcpyHostToDevice));
+    CK(launch_hash_pairs(a.p, b.p, c.p, count, nullptr));
+    CK(cudaMemcpy(out, c.p, 40 * count, cudaMemcpyDeviceToHost));
+    return TVMC_OK;
+}
+
+int tvmc_tip5_permutation_batch_gpu(uint64_t* d_states, size_t num_states, void* stream) {
+    CK(launch_tip5_permutations(d_states, num_states, as_stream(stream)));
+    return TVMC_OK;
+}
+
+int tvmc_tip5_permutation_batch_host(uint64_t* states, size_t num_states) {
+    if (num_states == 0) return TVMC_OK;
+    DBuf a;
+    CK(a.alloc(16 * num_states));
+    CK(cudaMemcpy(a.p, states, 128 * num_states, cudaMemcpyHostToDevice));
+    CK(launch_tip5_permutations(a.p, num_states, nullptr));
+    CK(cudaMemcpy(states, a.p, 128 * num_states, cudaMemcpyDeviceToHost));
+    return TVMC_OK;
+}
+
+// ---------------------------------------------------------------- Merkle
+
+int tvmc_merkle_tree_gpu(const uint64_t* d_leaves, uint64_t* d_tree, size_t num_leaves, void* stream) {
+    if (!is_pow2(num_leaves))
+        return fail(TVMC_ERR_INVALID, "Number of leaves must be a power of 2 (got %zu)", num_leaves);
+    CK(launch_merkle_tree(d_leaves, d_tree, num_leaves, LAYOUT_FLAT, as_stream(stream)));
+    return TVMC_OK;
+}
+
+int tvmc_merkle_root_gpu(const uint64_t* d_leaves, uint64_t* d_root, size_t num_leaves, void* stream) {
+    if (!is_pow2(num_leaves))
+        return fail(TVMC_ERR_INVALID, "Number of leaves must be a power of 2 (got %zu)", num_leaves);
+    cudaStream_t st = as_stream(stream);
+    uint64_t* tree = nullptr;
+    CK(cudaMallocAsync((void**)&tree, (2 * num_leaves - 1) * 40, st));
+    cudaError_t e = launch_merkle_tree(d_leaves, tree, num_leaves, LAYOUT_FLAT, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_root, tree + 5 * (2 * num_leaves - 2), 40, cudaMemcpyDeviceToDevice, st);
+    cudaFreeAsync(tree, st);
+    if (e != cudaSuccess) return cuda_fail(e, "merkle_root");
+    return TVMC_OK;
+}
+
+int tvmc_merkle_tree_heap_host(const uint64_t* leaves, size_t num_leaves, uint64_t* nodes) {
+    if (!is_pow2(num_leaves))
+        return fail(TVMC_ERR_INVALID, "Number of leaves must be a power of 2 (got %zu)", num_leaves);
+    DBuf a, t;
+    CK(a.alloc(5 * num_leaves));
+    CK(t.alloc(10 * num_leaves));
+    CK(cudaMemcpy(a.p, leaves, 40 * num_leaves, cudaMemcpyHostToDevice));
+    CK(cudaMemset(t.p, 0, 40));
+    CK(launch_merkle_tree(a.p, t.p, num_leaves, LAYOUT_HEAP, nullptr));
+    CK(cudaMemcpy(nodes, t.p, 80 * num_leaves, cudaMemcpyDeviceToHost));
+    return TVMC_OK;
+}
+
+// ---------------------------------------------------------------- commitment
+
+int tvmc_commit(const uint64_t* trace, size_t trace_len, size_t width, uint32_t expansion, uint64_t offset,
+                uint32_t flags, void* stream, tvmc_commitment** out) {
+    if (!out) return fail(TVMC_ERR_INVALID, "null output handle");
+    *out = nullptr;
+    if (!is_pow2(expansion) || expansion > 16)
+        return fail(TVMC_ERR_INVALID, "expansion factor %u is not a power of 2 <= 16", expansion);
+    if (flags & ~(TVMC_TRACE_DEVICE | TVMC_TRACE_ROW_MAJOR | TVMC_DISCARD_LDE | TVMC_SYNC | TVMC_PROFILE))
+        return fail(TVMC_ERR_INVALID, "unknown flag bits 0x%x", flags);
+    int logn, le;
+    int rc = check_lde_sizes(trace_len, trace_len * expansion, &logn, &le);
+    if (rc) return rc;
+    if (width && !trace) return fail(TVMC_ERR_INVALID, "null trace");
+    cudaStream_t st = as_stream(stream);
+    LdePlan pl;
+    if ((rc = get_plan(logn, le, offset, &pl))) return rc;
+
+    tvmc_commitment* c = new tvmc_commitment();
+    CK(cudaGetDevice(&c->device));
+    c->stream = st;
+    c->n = trace_len;
+    c->width = width;
+    c->L = trace_len * expansion;
+    auto bail = [&](int code) {
+        tvmc_commitment_free(c);
+        return code;
+    };
+    const size_t NW = trace_len * width;
+    if (cudaMalloc((void**)&c->d_nodes, 2 * c->L * 40) != cudaSuccess ||
+        (width && cudaMalloc((void**)&c->d_lde, c->L * width * 8) != cudaSuccess)) {
+        cudaGetLastError();
+        return bail(fail(TVMC_ERR_NOMEM, "cannot allocate LDE (%zu x %zu) and tree", c->L, width));
+    }
+    if (cudaMemsetAsync(c->d_nodes, 0, 40, st) != cudaSuccess) return bail(cuda_fail(cudaGetLastError(), "memset"));
+
+    const bool prof = flags & TVMC_PROFILE;
+    if (prof) {
+        for (auto& ev : c->prof)
+            if (cudaEventCreate(&ev) != cudaSuccess) return bail(cuda_fail(cudaGetLastError(), "event"));
+        cudaEventRecord(c->prof[0], st);
+    }
+    const bool dev = flags & TVMC_TRACE_DEVICE, rm = flags & TVMC_TRACE_ROW_MAJOR;
+    if (width && !dev && !rm) {
+        // host column-major trace: upload column chunks on a copy stream,
+        // overlapping the LDE of the previous chunk
+        if (prof) cudaEventRecord(c->prof[1], st);
+        rc = upload_lde_pipelined(pl, trace, trace_len, width, c->d_lde, c->L, st);
+        if (rc) return bail(rc);
+    } else if (width) {
+        const uint64_t* d_src = trace;
+        uint64_t* d_up = nullptr;
+        uint64_t* d_cm = nullptr;
+        cudaError_t e = cudaSuccess;
+        if (!dev) {
+            e = cudaMallocAsync((void**)&d_up, NW * 8, st);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(d_up, trace, NW * 8, cudaMemcpyHostToDevice, st);
+            d_src = d_up;
+        }
+        if (e == cudaSuccess && rm) {
+            e = cudaMallocAsync((void**)&d_cm, NW * 8, st);
+            if (e == cudaSuccess) e = launch_transpose(d_src, width, d_cm, trace_len, trace_len, width, st);
+            d_src = d_cm;
+        }
+        if (e != cudaSuccess) {
+            if (d_up) cudaFreeAsync(d_up, st);
+            if (d_cm) cudaFreeAsync(d_cm, st);
+            return bail(cuda_fail(e, "trace upload"));
+        }
+        if (prof) cudaEventRecord(c->prof[1], st);
+        rc = run_lde(pl, d_src, trace_len, c->d_lde, c->L, width, st);
+        if (d_up) cudaFreeAsync(d_up, st);
+        if (d_cm) cudaFreeAsync(d_cm, st);
+        if (rc) return bail(rc);
+    } else if (prof) {
+        cudaEventRecord(c->prof[1], st);
+    }
+    if (prof) cudaEventRecord(c->prof[2], st);
+    cudaError_t e = launch_hash_rows(c->d_lde, 1, c->L, c->L, (uint32_t)width, nullptr, c->d_nodes, LAYOUT_HEAP, st);
+    if (e != cudaSuccess) return bail(cuda_fail(e, "hash/merkle"));
+    if (prof) cudaEventRecord(c->prof[3], st);
+    if ((flags & TVMC_DISCARD_LDE) && c->d_lde) {
+        cudaFreeAsync(c->d_lde, st);  // stream-ordered after the hash kernel
+        c->d_lde = nullptr;
+    }
+    if (cudaEventCreateWithFlags(&c->done, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventRecord(c->done, st) != cudaSuccess)
+        return bail(cuda_fail(cudaGetLastError(), "event"));
+    if (flags & TVMC_SYNC) {
+        if (cudaEventSynchronize(c->done) != cudaSuccess) return bail(cuda_fail(cudaGetLastError(), "sync"));
+    }
+    *out = c;
+    return TVMC_OK;
+}
+
+int tvmc_commitment_sync(tvmc_commitment* c) {
+    if (!c) return fail(TVMC_ERR_INVALID, "null handle");
+    CK(cudaEventSynchronize(c->done));
+    return TVMC_OK;
+}
+
+int tvmc_commitment_root(tvmc_commitment* c, uint64_t* root) {
+    if (!c || !root) return fail(TVMC_ERR_INVALID, "null argument");
+    CK(cudaEventSynchronize(c->done));
+    CK(cudaMemcpy(root, c->d_nodes + 5, 40, cudaMemcpyDeviceToHost));
+    return TVMC_OK;
+}
+
+int tvmc_commitment_shape(const tvmc_commitment* c, size_t* lde_len, size_t* width) {
+    if (!c) return fail(TVMC_ERR_INVALID, "null handle");
+    if (lde_len) *lde_len = c->L;
+    if (width) *width = c->width;
+    return TVMC_OK;
+}
+
+int tvmc_commitment_device_lde(const tvmc_commitment* c, const uint64_t** d_lde) {
+    if (!c || !d_lde) return fail(TVMC_ERR_INVALID, "null argument");
+    *d_lde = c->d_lde;
+    return TVMC_OK;
+}
+
+int tvmc_commitment_device_tree(const tvmc_commitment* c, const uint64_t** d_nodes) {
+    if (!c || !d_nodes) return fail(TVMC_ERR_INVALID, "null argument");
+    *d_nodes = c->d_nodes;
+    return TVMC_OK;
+}
+
+int tvmc_commitment_auth_paths(tvmc_commitment* c, const size_t* leaf_idx, size_t count, uint64_t* out) {
+    if (!c) return fail(TVMC_ERR_INVALID, "null handle");
+    if (count == 0) return TVMC_OK;
+    for (size_t q = 0; q < count; q++)
+        if (leaf_idx[q] >= c->L) return fail(TVMC_ERR_RANGE, "Leaf index %zu out of range", leaf_idx[q]);
+    int h = log2u(c->L);
+    if (h == 0) return TVMC_OK;
+    std::vector<uint64_t> idx(leaf_idx, leaf_idx + count);
+    DBuf di, dout;
+    CK(di.alloc(count));
+    CK(dout.alloc(count * h * 5));
+    CK(cudaEventSynchronize(c->done));
+    CK(cudaMemcpy(di.p, idx.data(), count * 8, cudaMemcpyHostToDevice));
+    CK(launch_gather_auth_paths(c->d_nodes, c->L, LAYOUT_HEAP, di.p, count, dout.p, nullptr));
+    CK(cudaMemcpy(out, dout.p, count * h * 40, cudaMemcpyDeviceToHost));
+    return TVMC_OK;
+}
+
+int tvmc_auth_structure_indices(size_t num_leaves, const size_t* leaf_idx, size_t count, uint64_t* out,
+                                size_t max_out, size_t* num_out) {
+    if (!is_pow2(num_leaves)) return fail(TVMC_ERR_INVALID, "num_leaves must be a power of 2 (got %zu)", num_leaves);
+    std::vector<uint64_t> res;
+    int rc = auth_structure_nodes(num_leaves, leaf_idx, count, &res);
+    if (rc) return rc;
+    if (num_out) *num_out = res.size();
+    for (size_t i = 0; i < res.size() && i < max_out; i++) out[i] = res[i];
+    return TVMC_OK;
+}
+
+int tvmc_commitment_auth_structure(tvmc_commitment* c, const size_t* leaf_idx, size_t count, uint64_t* out,
+                                   size_t max_digests, size_t* num_digests) {
+    if (!c) return fail(TVMC_ERR_INVALID, "null handle");
+    const size_t n = c->L;
+    std::vector<uint64_t> res;
+    int rc = auth_structure_nodes(n, leaf_idx, count, &res);
+    if (rc) return rc;
+    if (num_digests) *num_digests = res.size();
+    size_t m = std::min(res.size(), max_digests);
+    if (m == 0) return TVMC_OK;
+    DBuf di, dout;
+    CK(di.alloc(m));
+    CK(dout.alloc(5 * m));
+    CK(cudaEventSynchronize(c->done));
+    CK(cudaMemcpy(di.p, res.data(), m * 8, cudaMemcpyHostToDevice));
+    CK(launch_gather_nodes(c->d_nodes, n, LAYOUT_HEAP, di.p, m, dout.p, nullptr));
+    CK(cudaMemcpy(out, dout.p, m * 40, cudaMemcpyDeviceToHost));
+    return TVMC_OK;
+}
+
+int tvmc_commitment_read_rows(tvmc_commitment* c, const size_t* rows, size_t count, uint64_t* out) {
+    if (!c) return fail(TVMC_ERR_INVALID, "null handle");
+    if (!c->d_lde && c->width) return fail(TVMC_ERR_INVALID, "LDE was discarded");
+    for (size_t q = 0; q < count; q++)
+        if (rows[q] >= c->L) return fail(TVMC_ERR_RANGE, "Row index %zu out of range", rows[q]);
+    if (count == 0 || c->width == 0) return TVMC_OK;
+    std::vector<uint64_t> idx(rows, rows + count);
+    DBuf di, dout;
+    CK(di.alloc(count));
+    CK(dout.alloc(count * c->width));
+    CK(cudaEventSynchronize(c->done));
+    CK(cudaMemcpy(di.p, idx.data(), count * 8, cudaMemcpyHostToDevice));
+    CK(launch_gather_rows(c->d_lde, c->L, (uint32_t)c->width, di.p, count, dout.p, nullptr));
+    CK(cudaMemcpy(out, dout.p, count * c->width * 8, cudaMemcpyDeviceToHost));
+    return TVMC_OK;
+}
+
+int tvmc_commitment_read_columns(tvmc_commitment* c, size_t col0, size_t ncols, uint64_t* out) {
+    if (!c) return fail(TVMC_ERR_INVALID, "null handle");
+    if (!c->d_lde && c->width) return fail(TVMC_ERR_INVALID, "LDE was discarded");
+    if (col0 > c->width || ncols > c->width - col0)
+        return fail(TVMC_ERR_RANGE, "columns [%zu, %zu) out of range", col0, col0 + ncols);
+    if (ncols == 0) return TVMC_OK;
+    CK(cudaEventSynchronize(c->done));
+    CK(cudaMemcpy(out, c->d_lde + col0 * c->L, ncols * c->L * 8, cudaMemcpyDeviceToHost));
+    return TVMC_OK;
+}
+
+int tvmc_commitment_read_lde(tvmc_commitment* c, uint64_t* out, int row_major) {
+    if (!c) return fail(TVMC_ERR_INVALID, "null handle");
+    if (!c->d_lde && c->width) return fail(TVMC_ERR_INVALID, "LDE was discarded");
+    if (c->width == 0) return TVMC_OK;
+    CK(cudaEventSynchronize(c->done));
+    const size_t W = c->L * c->width;
+    if (!row_major) {
+        CK(cudaMemcpy(out, c->d_lde, W * 8, cudaMemcpyDeviceToHost));
+        return TVMC_OK;
+    }
+    DBuf t;
+    CK(t.alloc(W));
+    CK(launch_transpose_cm_to_rm(c->d_lde, c->L, t.p, c->width, c->L, c->width, nullptr));
+    CK(cudaMemcpy(out, t.p, W * 8, cudaMemcpyDeviceToHost));
+    return TVMC_OK;
+}
+
+int tvmc_commitment_read_leaves(tvmc_commitment* c, uint64_t* out) {
+    if (!c) return fail(TVMC_ERR_INVALID, "null handle");
+    CK(cudaEventSynchronize(c->done));
+    CK(cudaMemcpy(out, c->d_nodes + 5 * c->L, c->L * 40, cudaMemcpyDeviceToHost));
+    return TVMC_OK;
+}
+
+int tvmc_commitment_read_nodes(tvmc_commitment* c, uint64_t* out) {
+    if (!c) return fail(TVMC_ERR_INVALID, "null handle");
+    CK(cudaEventSynchronize(c->done));
+    CK(cudaMemcpy(out, c->d_nodes, 2 * c->L * 40, cudaMemcpyDeviceToHost));
+    return TVMC_OK;
+}
+
+int tvmc_commitment_free(tvmc_commitment* c) {
+    if (!c) return TVMC_OK;
+    if (c->done) {
+        cudaEventSynchronize(c->done);
+        cudaEventDestroy(c->done);
+    } else if (c->stream || true) {
+        cudaStreamSynchronize(c->stream);
+    }
+    for (auto ev : c->prof)
+        if (ev) cudaEventDestroy(ev);
+    if (c->d_lde) cudaFree(c->d_lde);
+    if (c->d_nodes) cudaFree(c->d_nodes);
+    delete c;
+    return TVMC_OK;
+}
+
+int tvmc_commitment_phase_ms(tvmc_commitment* c, float* ms) {
+    if (!c || !ms) return fail(TVMC_ERR_INVALID, "null argument");
+    if (!c->prof[0]) return fail(TVMC_ERR_INVALID, "commitment was not made with TVMC_PROFILE");
+    CK(cudaEventSynchronize(c->done));
+    for (int i = 0; i < 3; i++) CK(cudaEventElapsedTime(&ms[i], c->prof[i], c->prof[i + 1]));
+    return TVMC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,299 @@
+// Tip5 row hashing and Merkle tree kernels (sm_100a).
+//
+// Row hash: one LDE row per thread, the 16-word sponge state in registers,
+// the next 10-element chunk prefetched into registers while the current one is
+// permuted.  Rows are read column-major (a warp reads 32 consecutive rows of
+// one column, 256 contiguous bytes).  Semantics: Tip5::hash_varlen
+// (src/hash/tip5.cpp:246-282) -- zero state, overwrite the rate with each full
+// chunk and permute, last chunk = rest, 1, zeros.
+//
+// Merkle: parent = hash_pair(left, right) (src/merkle/merkle_tree.cpp:41-61).
+// The lowest log2(blockDim) levels are built in shared memory inside the row
+// hash kernel itself; the remaining levels take one launch per 8 levels.
+#include "internal.cuh"
+#include "tip5.cuh"
+
+namespace tvmc {
+
+constexpr int HASH_THREADS = 128;
+constexpr int UP_THREADS = 128;
+
+__device__ __forceinline__ void store_digest(uint64_t* p, const uint64_t d[5]) {
+#pragma unroll
+    for (int i = 0; i < 5; i++) p[i] = d[i];
+}
+
+// Builds `levels` tree levels above the `count` digests held in sd (count =
+// blockDim.x), where those digests are heap nodes [base, base + count).
+__device__ __forceinline__ void subtree_levels(uint64_t* sd, uint64_t base, int levels, uint64_t* tree,
+                                               uint64_t n, int layout, const uint32_t* lt) {
+    int count = blockDim.x;
+    for (int lv = 1; lv <= levels; lv++) {
+        count >>= 1;
+        base >>= 1;
+        uint64_t h[5];
+        bool act = threadIdx.x < count;
+        if (act) t5_hash_pair(sd + 10 * threadIdx.x, sd + 10 * threadIdx.x + 5, h, lt);
+        __syncthreads();
+        if (act) {
+            store_digest(sd + 5 * threadIdx.x, h);
+            store_digest(tree + 5 * node_slot(base + threadIdx.x, n, layout), h);
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(HASH_THREADS) k_hash_rows(
+    const uint64_t* __restrict__ tab, uint64_t rstride, uint64_t cstride, uint64_t rows, uint32_t width,
+    uint64_t* __restrict__ digests, uint64_t* __restrict__ tree, int layout, int fuse) {
+    __shared__ uint32_t sbox[T5_SBOX_WORDS];
+    __shared__ uint64_t sd[HASH_THREADS * 5];
+    t5_sbox_init(sbox);
+    __syncthreads();
+    const uint32_t* lt = sbox + (threadIdx.x & 31);
+
+    const uint64_t row = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = row < rows;
+    const uint64_t* p = tab + (live ? row : 0) * rstride;
+
+    uint64_t s[T5_STATE];
+#pragma unroll
+    for (int i = 0; i < T5_STATE; i++) s[i] = 0;
+
+    const uint32_t full = width / T5_RATE;
+    const uint32_t rem = width - full * T5_RATE;
+    uint64_t nx[T5_RATE];
+    // prefetch chunk 0 (or the padded tail if there is no full chunk)
+#pragma unroll
+    for (int i = 0; i < T5_RATE; i++) {
+        uint32_t c = (uint32_t)i;
+        nx[i] = (live && (full > 0 || c < rem)) ? __ldg(p + (uint64_t)c * cstride) : 0;
+    }
+    for (uint32_t k = 0; k < full; k++) {
+#pragma unroll
+        for (int i = 0; i < T5_RATE; i++) s[i] = nx[i];
+        // prefetch the next chunk (full or tail)
+        uint32_t c0 = (k + 1) * T5_RATE;
+        uint32_t lim = (k + 1 < full) ? T5_RATE : rem;
+#pragma unroll
+        for (int i = 0; i < T5_RATE; i++)
+            nx[i] = (live && (uint32_t)i < lim) ? __ldg(p + (uint64_t)(c0 + i) * cstride) : 0;
+        t5_permutation(s, lt);
+    }
+#pragma unroll
+    for (int i = 0; i < T5_RATE; i++) s[i] = ((uint32_t)i < rem) ? nx[i] : ((uint32_t)i == rem ? 1 : 0);
+    t5_permutation(s, lt);
+
+    uint64_t d[5];
+#pragma unroll
+    for (int i = 0; i < 5; i++) d[i] = gl_canon(s[i]);
+
+    if (tree == nullptr) {
+        if (live) store_digest(digests + 5 * row, d);
+        return;
+    }
+    // rows is a power of two and a multiple of blockDim here
+    store_digest(tree + 5 * node_slot(rows + row, rows, layout), d);
+    if (fuse > 0) {
+        store_digest(sd + 5 * threadIdx.x, d);
+        __syncthreads();
+        subtree_levels(sd, rows + (uint64_t)blockIdx.x * blockDim.x, fuse, tree, rows, layout, lt);
+    }
+}
+
+// One launch builds up to `levels` levels above the level of m nodes.
+__global__ void __launch_bounds__(UP_THREADS) k_merkle_up(uint64_t* __restrict__ tree, uint64_t n,
+                                                          uint64_t m, int layout, int levels) {
+    __shared__ uint32_t sbox[T5_SBOX_WORDS];
+    __shared__ uint64_t sd[UP_THREADS * 5];
+    t5_sbox_init(sbox);
+    __syncthreads();
+    const uint32_t* lt = sbox + (threadIdx.x & 31);
+    // parents of this block: heap nodes [m/2 + blockIdx.x*blockDim.x, +blockDim.x)
+    uint64_t par = (m >> 1) + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t* l = tree + 5 * node_slot(2 * par, n, layout);
+    const uint64_t* r = tree + 5 * node_slot(2 * par + 1, n, layout);
+    uint64_t a[5], b[5], h[5];
+#pragma unroll
+    for (int i = 0; i < 5; i++) { a[i] = l[i]; b[i] = r[i]; }
+    t5_hash_pair(a, b, h, lt);
+    store_digest(tree + 5 * node_slot(par, n, layout), h);
+    if (levels > 1) {
+        store_digest(sd + 5 * threadIdx.x, h);
+        __syncthreads();
+        subtree_levels(sd, par - threadIdx.x, levels - 1, tree, n, layout, lt);
+    }
+}
+
+__global__ void k_copy_leaves(const uint64_t* __restrict__ leaves, uint64_t* __restrict__ tree, uint64_t n,
+                              int layout) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint64_t* dst = tree + 5 * node_slot(n + i, n, layout);
+#pragma unroll
+    for (int k = 0; k < 5; k++) dst[k] = gl_canon(leaves[5 * i + k]);
+}
+
+__global__ void __launch_bounds__(128) k_hash_pairs(const uint64_t* __restrict__ left,
+                                                    const uint64_t* __restrict__ right,
+                                                    uint64_t* __restrict__ out, uint64_t count) {
+    __shared__ uint32_t sbox[T5_SBOX_WORDS];
+    t5_sbox_init(sbox);
+    __syncthreads();
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    uint64_t a[5], b[5], h[5];
+#pragma unroll
+    for (int k = 0; k < 5; k++) { a[k] = left[5 * i + k]; b[k] = right[5 * i + k]; }
+    t5_hash_pair(a, b, h, sbox + (threadIdx.x & 31));
+    store_digest(out + 5 * i, h);
+}
+
+__global__ void __launch_bounds__(128) k_tip5_perm(uint64_t* __restrict__ states, uint64_t count) {
+    __shared__ uint32_t sbox[T5_SBOX_WORDS];
+    t5_sbox_init(sbox);
+    __syncthreads();
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    uint64_t s[T5_STATE];
+#pragma unroll
+    for (int k = 0; k < T5_STATE; k++) s[k] = states[16 * i + k];
+    t5_permutation(s, sbox + (threadIdx.x & 31));
+#pragma unroll
+    for (int k = 0; k < T5_STATE; k++) states[16 * i + k] = gl_canon(s[k]);
+}
+
+__global__ void k_gather_auth(const uint64_t* __restrict__ tree, uint64_t n, int layout, int height,
+                              const uint64_t* __restrict__ idx, uint64_t count, uint64_t* __restrict__ out) {
+    uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count * (uint64_t)height) return;
+    uint64_t q = t / height;
+    int k = (int)(t - q * height);
+    uint64_t node = ((n + idx[q]) >> k) ^ 1;
+    const uint64_t* src = tree + 5 * node_slot(node, n, layout);
+#pragma unroll
+    for (int i = 0; i < 5; i++) out[5 * t + i] = src[i];
+}
+
+__global__ void k_gather_nodes(const uint64_t* __restrict__ tree, uint64_t n, int layout,
+                               const uint64_t* __restrict__ hidx, uint64_t count, uint64_t* __restrict__ out) {
+    uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    const uint64_t* src = tree + 5 * node_slot(hidx[t], n, layout);
+#pragma unroll
+    for (int i = 0; i < 5; i++) out[5 * t + i] = src[i];
+}
+
+__global__ void k_gather_rows(const uint64_t* __restrict__ tab, uint64_t ld, uint32_t width,
+                              const uint64_t* __restrict__ rows, uint64_t count, uint64_t* __restrict__ out) {
+    uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count * (uint64_t)width) return;
+    uint64_t q = t / width;
+    uint64_t c = t - q * width;
+    out[t] = tab[c * ld + rows[q]];
+}
+
+static inline int ilog2u(uint64_t x) { return 63 - __builtin_clzll(x); }
+
+static inline unsigned grid_for(uint64_t work, unsigned threads) {
+    return (unsigned)((work + threads - 1) / threads);
+}
+
+cudaError_t launch_merkle_from_leaves(uint64_t* tree, uint64_t n, int layout, cudaStream_t st) {
+    // n leaves already in place; build all levels above.
+    uint64_t m = n;
+    while (m > 1) {
+        uint64_t parents = m >> 1;
+        unsigned threads = (unsigned)(parents < UP_THREADS ? parents : UP_THREADS);
+        int levels = ilog2u(threads) + 1;
+        count_launch();
+        k_merkle_up<<<grid_for(parents, threads), threads, 0, st>>>(tree, n, m, layout, levels);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        m >>= levels;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t launch_hash_rows(const uint64_t* table, uint64_t rstride, uint64_t cstride, uint64_t rows,
+                             uint32_t width, uint64_t* digests, uint64_t* tree, int layout,
+                             cudaStream_t st) {
+    if (rows == 0) return cudaSuccess;
+    if (tree == nullptr) {
+        count_launch();
+        k_hash_rows<<<grid_for(rows, HASH_THREADS), HASH_THREADS, 0, st>>>(table, rstride, cstride, rows, width,
+                                                                           digests, nullptr, layout, 0);
+        return cudaGetLastError();
+    }
+    unsigned threads = (unsigned)(rows < HASH_THREADS ? rows : HASH_THREADS);
+    int fuse = ilog2u(threads);
+    count_launch();
+    k_hash_rows<<<grid_for(rows, threads), threads, 0, st>>>(table, rstride, cstride, rows, width, nullptr, tree,
+                                                             layout, fuse);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    // the block subtrees are complete; continue from the level of rows/threads nodes
+    uint64_t m = rows / threads;
+    while (m > 1) {
+        uint64_t parents = m >> 1;
+        unsigned th = (unsigned)(parents < UP_THREADS ? parents : UP_THREADS);
+        int levels = ilog2u(th) + 1;
+        count_launch();
+        k_merkle_up<<<grid_for(parents, th), th, 0, st>>>(tree, rows, m, layout, levels);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        m >>= levels;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t launch_merkle_tree(const uint64_t* leaves, uint64_t* tree, uint64_t n, int layout,
+                               cudaStream_t st) {
+    count_launch();
+    k_copy_leaves<<<grid_for(n, 256), 256, 0, st>>>(leaves, tree, n, layout);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return launch_merkle_from_leaves(tree, n, layout, st);
+}
+
+cudaError_t launch_hash_pairs(const uint64_t* left, const uint64_t* right, uint64_t* out, uint64_t count,
+                              cudaStream_t st) {
+    if (count == 0) return cudaSuccess;
+    count_launch();
+    k_hash_pairs<<<grid_for(count, 128), 128, 0, st>>>(left, right, out, count);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tip5_permutations(uint64_t* states, uint64_t count, cudaStream_t st) {
+    if (count == 0) return cudaSuccess;
+    count_launch();
+    k_tip5_perm<<<grid_for(count, 128), 128, 0, st>>>(states, count);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gather_auth_paths(const uint64_t* tree, uint64_t n, int layout, const uint64_t* idx,
+                                     uint64_t count, uint64_t* out, cudaStream_t st) {
+    int height = ilog2u(n);
+    if (count == 0 || height == 0) return cudaSuccess;
+    count_launch();
+    k_gather_auth<<<grid_for(count * height, 256), 256, 0, st>>>(tree, n, layout, height, idx, count, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gather_nodes(const uint64_t* tree, uint64_t n, int layout, const uint64_t* heap_idx,
+                                uint64_t count, uint64_t* out, cudaStream_t st) {
+    if (count == 0) return cudaSuccess;
+    count_launch();
+    k_gather_nodes<<<grid_for(count, 256), 256, 0, st>>>(tree, n, layout, heap_idx, count, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gather_rows(const uint64_t* table, uint64_t ld, uint32_t width, const uint64_t* rows,
+                               uint64_t count, uint64_t* out, cudaStream_t st) {
+    if (count == 0 || width == 0) return cudaSuccess;
+    count_launch();
+    k_gather_rows<<<grid_for(count * width, 256), 256, 0, st>>>(table, ld, width, rows, count, out);
+    return cudaGetLastError();
+}
+
+}  // namespace tvmc

@@ -1,0 +1,92 @@
+// Internal launcher declarations shared by the CUDA translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstddef>
+
+namespace tvmc {
+
+// Number of kernels this library has launched (all devices, all threads).
+void count_launch();
+
+// Merkle node storage layouts.
+//   HEAP: 2n digests, node h at h (root 1, leaves [n, 2n), slot 0 unused) --
+//         the reference's CPU MerkleTree (src/merkle/merkle_tree.cpp:12-33).
+//   FLAT: 2n-1 digests, [leaves | level 1 | ... | root] -- the reference's
+//         GPU merkle_tree_gpu layout (src/gpu/kernels/merkle_kernel.cu:41-105).
+enum NodeLayout : int { LAYOUT_HEAP = 0, LAYOUT_FLAT = 1 };
+
+__host__ __device__ inline uint64_t node_slot(uint64_t h, uint64_t n, int layout) {
+    if (layout == LAYOUT_HEAP) return h;
+    // h lies on the level with 2^m nodes; that level starts at 2n - 2^(m+1) in FLAT.
+#ifdef __CUDA_ARCH__
+    uint64_t pm = 1ull << (63 - __clzll((long long)h));
+#else
+    uint64_t pm = 1ull << (63 - __builtin_clzll(h));
+#endif
+    return 2 * n + h - 3 * pm;
+}
+
+// ---- hash.cu -------------------------------------------------------------
+// Leaf digests of `rows` rows; element (r, c) at table[r*rstride + c*cstride].
+// If `tree` is non-null, rows must be a power of two: leaves are written as
+// tree nodes (layout) and the whole tree is completed up to the root.
+// Otherwise digests go to `digests` (rows x 5).
+cudaError_t launch_hash_rows(const uint64_t* table, uint64_t rstride, uint64_t cstride, uint64_t rows,
+                             uint32_t width, uint64_t* digests, uint64_t* tree, int layout,
+                             cudaStream_t st);
+// Complete a tree whose leaf level (n leaves) is already stored in `tree`.
+cudaError_t launch_merkle_from_leaves(uint64_t* tree, uint64_t n, int layout, cudaStream_t st);
+// Copy n leaf digests into the tree's leaf slots and complete the tree.
+cudaError_t launch_merkle_tree(const uint64_t* leaves, uint64_t* tree, uint64_t n, int layout,
+                               cudaStream_t st);
+cudaError_t launch_hash_pairs(const uint64_t* left, const uint64_t* right, uint64_t* out, uint64_t count,
+                              cudaStream_t st);
+cudaError_t launch_tip5_permutations(uint64_t* states, uint64_t count, cudaStream_t st);
+// out[q*height + k] = sibling of the k-th ancestor of leaf idx[q] (k = 0 is the leaf's sibling).
+cudaError_t launch_gather_auth_paths(const uint64_t* tree, uint64_t n, int layout, const uint64_t* idx,
+                                     uint64_t count, uint64_t* out, cudaStream_t st);
+cudaError_t launch_gather_nodes(const uint64_t* tree, uint64_t n, int layout, const uint64_t* heap_idx,
+                                uint64_t count, uint64_t* out, cudaStream_t st);
+// Rows of a column-major table (col stride ld) gathered row-major: out[q*width + c].
+cudaError_t launch_gather_rows(const uint64_t* table, uint64_t ld, uint32_t width, const uint64_t* rows,
+                               uint64_t count, uint64_t* out, cudaStream_t st);
+
+// ---- ntt.cu --------------------------------------------------------------
+struct NttTables;  // device twiddle tables, owned by api.cu's per-device cache
+
+// Twiddle bundle for one transform size / LDE configuration.
+struct LdePlan {
+    int logn;             // trace length N = 2^logn
+    int log_exp;          // expansion E = 2^log_exp
+    uint64_t offset;      // coset offset of the evaluation domain
+    const uint64_t* tw12_f;   // w_4096^m, m < 2048 (forward sub-DFT twiddles)
+    const uint64_t* tw12_i;   // inverse of the above
+    const uint64_t* wn_f_lo;  // w_N^(e & 4095)
+    const uint64_t* wn_f_hi;  // w_N^((e >> 12) * 4096)
+    const uint64_t* wn_i_lo;  // same for w_N^-1
+    const uint64_t* wn_i_hi;
+    const uint64_t* sc_lo;    // E tables of 4096: s_c^(i & 4095), s_c = offset * w_{EN}^c
+    const uint64_t* sc_hi;    // E tables of max(1, N/4096): N^-1 * s_c^((i >> 12) * 4096)
+};
+
+// Batched LDE of `cols` column-major columns: trace[c*tld + r] (r < N) ->
+// out[c*old + r] (r < E*N).  scratch must hold scratch_words_lde(...) words.
+size_t lde_scratch_words(int logn, int log_exp, uint64_t cols);
+cudaError_t launch_lde(const LdePlan& pl, const uint64_t* trace, uint64_t tld, uint64_t* out, uint64_t old,
+                       uint64_t cols, uint64_t* scratch, cudaStream_t st);
+// Batched NTT in place on column-major data[c*ld + r], r < 2^logn.
+size_t ntt_scratch_words(int logn, uint64_t cols);
+cudaError_t launch_ntt(const LdePlan& pl, int inverse, uint64_t* data, uint64_t ld, uint64_t cols,
+                       uint64_t* scratch, cudaStream_t st);
+// Row-major (rows x cols, row stride rld) -> column-major (col stride cld).
+cudaError_t launch_transpose(const uint64_t* in, uint64_t rld, uint64_t* out, uint64_t cld, uint64_t rows,
+                             uint64_t cols, cudaStream_t st);
+// Column-major -> row-major.
+cudaError_t launch_transpose_cm_to_rm(const uint64_t* in, uint64_t cld, uint64_t* out, uint64_t rld,
+                                      uint64_t rows, uint64_t cols, cudaStream_t st);
+
+constexpr int MAX_LOG_NTT = 24;       // plain NTT sizes up to 2^24
+constexpr int MAX_LOG_LDE_TRACE = 22; // LDE trace lengths up to 2^22
+
+}  // namespace tvmc

@@ -1,0 +1,161 @@
+// Tip5 permutation for sm_100a, one sponge state per thread held in registers.
+//
+// Semantics follow the reference's Tip5 (src/hash/tip5.cpp:92-203): 16-word
+// state, 5 rounds of [S-box -> MDS -> round constants].  The S-box applies
+// split-and-lookup to words 0-3 (to Montgomery form, byte-wise table, back)
+// and x^7 to words 4-15; the MDS is the circulant matrix whose first column is
+// given below.  The byte table is the offset Fermat cube map x -> (x+1)^3 - 1
+// over F_257, generated here rather than tabulated.
+//
+// B200 layout choices:
+//   * the byte table lives in shared memory as 64 words x 32 lanes, every lane
+//     owning its own bank, so the 8 lookups per word never conflict;
+//   * the MDS is computed exactly in integers: each word is split into 32-bit
+//     halves and the circulant products accumulate in 64-bit registers
+//     (coefficients < 2^16, sums < 2^52), then the two halves are recombined
+//     with one 128-bit reduction per output word.
+#pragma once
+#include <cstdint>
+#include "field.cuh"
+
+namespace tvmc {
+
+constexpr int T5_STATE = 16;
+constexpr int T5_RATE = 10;
+constexpr int T5_ROUNDS = 5;
+
+// Circulant MDS first column and round constants of Tip5 (published
+// parameters; identical to src/hash/tip5.cpp:27-79).
+__device__ __constant__ uint32_t c_t5_mds[T5_STATE] = {
+    61402, 1108, 28750, 33823, 7454, 43244, 53865, 12034,
+    56951, 27521, 41351, 40901, 12021, 59689, 26798, 17845};
+
+__device__ __constant__ uint64_t c_t5_rc[T5_ROUNDS * T5_STATE] = {
+    0xBD2A3DEB61AB60DEull, 0xEA7DF21AD9547ED2ull, 0x900B3677A1DE063Full, 0x1B46887E876C8677ull,
+    0xD364D977889CFB97ull, 0xDC8DFAC843699F02ull, 0x375C405D7190DB58ull, 0x27924006D2B0D4B1ull,
+    0x78DD1172D483CD38ull, 0x3346C66244882A56ull, 0xB0249B279F498AA5ull, 0x94CD51BE79338D4Dull,
+    0xB0E0DC7052C5B218ull, 0xF8DCC4D248ADAD95ull, 0x68E3C635FEC868B7ull, 0xD7D06B3FFB6B0D8Cull,
+    0xF3500DEA20EF032Aull, 0x4865BF175BBA5803ull, 0xD5F7FE3027287A27ull, 0xA57333F44E193412ull,
+    0x8726E153A977EAE2ull, 0x3014A98463FC191Bull, 0xBA145461AF39B212ull, 0x03AB70105933202Full,
+    0x3D90B7EEBFCF71E5ull, 0x386322B1CC520BFDull, 0x27C2C8DAF774F675ull, 0x4FCB83F50309BC6Aull,
+    0x5E6D5CE8275F3CB3ull, 0xECC2F6592C8F905Cull, 0x837F532461E609B4ull, 0xB2B1F6B95C92C93Cull,
+    0xC0027AF556411DC1ull, 0x16E18C885FC2A26Cull, 0x8880EF183D9F2BF3ull, 0xB2930BDB5CA88C45ull,
+    0x9C2EC8322E1C1553ull, 0xE5B05EAF3220A674ull, 0xA49CC6AE4B861C4Eull, 0x11708E0AEB86EBD7ull,
+    0xC09DE92BBC3902E0ull, 0x929B3C79516BCBC1ull, 0xE006E5BF738F27D1ull, 0x2D9E1EC0EAC8EA38ull,
+    0x0984D8D94BF937C5ull, 0x4959273C220E6747ull, 0xFE1D934207E796FAull, 0x2B9B9298F2F6DD73ull,
+    0x07A1F5A67D6E3A41ull, 0x4407593EE73743D9ull, 0x9F054720EF802E59ull, 0x78D4B711336E6AA6ull,
+    0xADC638AEF3C8B228ull, 0xA4D6D3E86AFB2114ull, 0x9D4808E725531968ull, 0x369804DF3866D0EFull,
+    0xE6DBD9A9D2215024ull, 0x8ED22CA212EE85B2ull, 0x397BB882FCD23EB6ull, 0xEB8F8786D7277531ull,
+    0x9999D4CDAFF543B5ull, 0xF382A61217F192D6ull, 0x49C37260B026ADC1ull, 0x3FF8918CE35C1019ull,
+    0x2E7DF8B76080BD07ull, 0xF5DBAC250B8A28B9ull, 0x853C3727AE9DA4CCull, 0xB2F1F5F3D9E5A26Dull,
+    0x3FCE22012D337847ull, 0x6B5A3E6DB7EEE347ull, 0x171582CD59DDE50Dull, 0xC0C0B3095EE62A8Aull,
+    0x665B25C6F6A203D2ull, 0x3099AED93B6AE69Full, 0x801DF6092BE69C38ull, 0x8066AD0CDFFF43CDull,
+    0x8AF9D44A5F4FDC6Bull, 0xD80219CD97C0D762ull, 0x10C9CEBA14148EBBull, 0x539BD4C3F2F24474ull};
+
+// Shared-memory S-box table: word w of lane l holds table bytes 4w..4w+3.
+constexpr int T5_SBOX_WORDS = 64 * 32;
+
+// Fill the lane-replicated byte table; call from all threads, then sync.
+__device__ __forceinline__ void t5_sbox_init(uint32_t* tbl) {
+    for (int i = threadIdx.x; i < T5_SBOX_WORDS; i += blockDim.x) {
+        int w = i >> 5;
+        uint32_t v = 0;
+        for (int b = 0; b < 4; b++) {
+            int x = 4 * w + b + 1;
+            int c = (x * x % 257) * x % 257;
+            v |= (uint32_t)((c + 256) % 257) << (8 * b);
+        }
+        tbl[i] = v;
+    }
+}
+
+// Byte-wise S-box of a 32-bit word through the lane's private table column.
+__device__ __forceinline__ uint32_t t5_lookup32(uint32_t m, const uint32_t* lane_tbl) {
+    uint32_t w0 = lane_tbl[((m >> 2) & 63) << 5];
+    uint32_t w1 = lane_tbl[((m >> 10) & 63) << 5];
+    uint32_t w2 = lane_tbl[((m >> 18) & 63) << 5];
+    uint32_t w3 = lane_tbl[((m >> 26) & 63) << 5];
+    // byte k of the result = byte (m_k & 3) of w_k
+    uint32_t lo = __byte_perm(w0, w1, (m & 3) | (((m >> 8) & 3) + 4) << 4);
+    uint32_t hi = __byte_perm(w2, w3, ((m >> 16) & 3) | (((m >> 24) & 3) + 4) << 4);
+    return __byte_perm(lo, hi, 0x5410);
+}
+
+// split_and_lookup (src/hash/tip5.cpp:119-145) for any representative x.
+__device__ __forceinline__ uint64_t t5_split_lookup(uint64_t x, const uint32_t* lane_tbl) {
+    // Montgomery form x * 2^64 mod p = x0*(2^32-1) - x1 (mod p), always canonical.
+    uint64_t x0 = x & GL_EPS, x1 = x >> 32;
+    uint64_t t = (x0 << 32) - x0;
+    uint64_t m = t - x1;
+    if (t < x1) m -= GL_EPS;
+    uint32_t lo = t5_lookup32((uint32_t)m, lane_tbl);
+    uint32_t hi = t5_lookup32((uint32_t)(m >> 32), lane_tbl);
+    uint64_t y = ((uint64_t)hi << 32) | lo;
+    // back from Montgomery form: y * 2^-64 mod p, canonical.
+    uint64_t sh = y << 32;
+    uint64_t a = y + sh;
+    uint64_t b = a - (a >> 32) - (uint64_t)(a < y);
+    return b ? GL_P - b : 0;
+}
+
+__device__ __forceinline__ uint64_t t5_pow7(uint64_t x) {
+    uint64_t x2 = gl_sqr(x);
+    uint64_t x3 = gl_mul(x, x2);
+    uint64_t x4 = gl_sqr(x2);
+    return gl_mul(x3, x4);
+}
+
+// Circulant MDS: out[r] = sum_c M[(r - c) mod 16] * s[c] (mod p).
+__device__ __forceinline__ void t5_mds(uint64_t s[T5_STATE]) {
+    uint64_t lo[T5_STATE], hi[T5_STATE];
+#pragma unroll
+    for (int r = 0; r < T5_STATE; r++) { lo[r] = 0; hi[r] = 0; }
+#pragma unroll
+    for (int c = 0; c < T5_STATE; c++) {
+        uint32_t l = (uint32_t)s[c], h = (uint32_t)(s[c] >> 32);
+#pragma unroll
+        for (int r = 0; r < T5_STATE; r++) {
+            uint32_t m = c_t5_mds[(r - c) & 15];
+            lo[r] += (uint64_t)m * l;
+            hi[r] += (uint64_t)m * h;
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < T5_STATE; r++) {
+        // value = lo + hi * 2^32 as a 128-bit number (sh:sl), sh < 2^21.
+        uint64_t sl = lo[r] + (hi[r] << 32);
+        uint64_t sh = (hi[r] >> 32) + (uint64_t)(sl < lo[r]);
+        uint64_t v = sh * GL_EPS;       // < 2^53
+        uint64_t x = sl + v;
+        if (x < v) x += GL_EPS;
+        s[r] = x;
+    }
+}
+
+__device__ __forceinline__ void t5_permutation(uint64_t s[T5_STATE], const uint32_t* lane_tbl) {
+#pragma unroll 1
+    for (int rnd = 0; rnd < T5_ROUNDS; rnd++) {
+#pragma unroll
+        for (int i = 0; i < 4; i++) s[i] = t5_split_lookup(s[i], lane_tbl);
+#pragma unroll
+        for (int i = 4; i < T5_STATE; i++) s[i] = t5_pow7(s[i]);
+        t5_mds(s);
+#pragma unroll
+        for (int i = 0; i < T5_STATE; i++) s[i] = gl_add_pc(s[i], c_t5_rc[rnd * T5_STATE + i]);
+    }
+}
+
+// Tip5::hash_pair / hash_10: rate = left || right, capacity = 1s.
+__device__ __forceinline__ void t5_hash_pair(const uint64_t l[5], const uint64_t r[5], uint64_t out[5],
+                                             const uint32_t* lane_tbl) {
+    uint64_t s[T5_STATE];
+#pragma unroll
+    for (int i = 0; i < 5; i++) { s[i] = l[i]; s[5 + i] = r[i]; }
+#pragma unroll
+    for (int i = T5_RATE; i < T5_STATE; i++) s[i] = 1;
+    t5_permutation(s, lane_tbl);
+#pragma unroll
+    for (int i = 0; i < 5; i++) out[i] = gl_canon(s[i]);
+}
+
+}  // namespace tvmc

@@ -1,0 +1,366 @@
+"""Python binding of the tvmc C ABI (include/tvmc.h) via ctypes.
+
+This is a thin host-side mirror of the reference's operator interfaces for the
+table-commitment path (NTT / LDE / Tip5 / MerkleTree / table commitment).  It
+loads the in-tree libtvmc.so and raises if it is missing: there is no CPU
+fallback.  Host-buffer functions take numpy arrays; the *_gpu functions take
+device pointers (ints), e.g. torch.Tensor.data_ptr().
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libtvmc.so")
+P = 0xFFFFFFFF00000001
+
+OK, ERR_INVALID, ERR_RANGE, ERR_NOMEM, ERR_CUDA, ERR_TIMEOUT, ERR_UNSUPPORTED = range(7)
+
+TRACE_DEVICE = 0x1
+TRACE_ROW_MAJOR = 0x2
+DISCARD_LDE = 0x4
+SYNC = 0x8
+PROFILE = 0x10
+
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+_szp = ctypes.POINTER(ctypes.c_size_t)
+_vp = ctypes.c_void_p
+_sz = ctypes.c_size_t
+
+
+class TvmcError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"tvmc status {status}: {msg}")
+        self.status = status
+
+
+class InvalidArgument(TvmcError, ValueError):
+    pass
+
+
+class OutOfRange(TvmcError, IndexError):
+    pass
+
+
+def build() -> None:
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+# Every exported symbol and its (restype, argtypes).
+SIGNATURES = {
+    "tvmc_last_error": (ctypes.c_char_p, []),
+    "tvmc_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "tvmc_version": (ctypes.c_int, []),
+    "tvmc_device_count": (ctypes.c_int, []),
+    "tvmc_ntt_forward_batched_gpu": (ctypes.c_int, [_vp, _sz, _sz, _vp]),
+    "tvmc_ntt_inverse_batched_gpu": (ctypes.c_int, [_vp, _sz, _sz, _vp]),
+    "tvmc_ntt_host": (ctypes.c_int, [_u64p, _sz, _sz, ctypes.c_int]),
+    "tvmc_lde_batch_gpu": (ctypes.c_int, [_vp, _sz, _sz, _vp, _sz, ctypes.c_uint64, ctypes.c_uint64, _vp]),
+    "tvmc_lde_host": (ctypes.c_int, [_u64p, _sz, _sz, _u64p, _sz, ctypes.c_uint64]),
+    "tvmc_hash_bfield_rows_gpu": (ctypes.c_int, [_vp, _sz, _sz, _vp, _vp]),
+    "tvmc_hash_xfield_rows_gpu": (ctypes.c_int, [_vp, _sz, _sz, _vp, _vp]),
+    "tvmc_hash_varlen_host": (ctypes.c_int, [_u64p, _sz, _sz, _u64p]),
+    "tvmc_hash_pairs_gpu": (ctypes.c_int, [_vp, _vp, _vp, _sz, _vp]),
+    "tvmc_hash_pairs_host": (ctypes.c_int, [_u64p, _u64p, _u64p, _sz]),
+    "tvmc_tip5_permutation_batch_gpu": (ctypes.c_int, [_vp, _sz, _vp]),
+    "tvmc_tip5_permutation_batch_host": (ctypes.c_int, [_u64p, _sz]),
+    "tvmc_merkle_tree_gpu": (ctypes.c_int, [_vp, _vp, _sz, _vp]),
+    "tvmc_merkle_root_gpu": (ctypes.c_int, [_vp, _vp, _sz, _vp]),
+    "tvmc_merkle_tree_heap_host": (ctypes.c_int, [_u64p, _sz, _u64p]),
+    "tvmc_commit": (ctypes.c_int, [_vp, _sz, _sz, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint32, _vp,
+                                   ctypes.POINTER(_vp)]),
+    "tvmc_commitment_root": (ctypes.c_int, [_vp, _u64p]),
+    "tvmc_commitment_sync": (ctypes.c_int, [_vp]),
+    "tvmc_commitment_shape": (ctypes.c_int, [_vp, _szp, _szp]),
+    "tvmc_commitment_device_lde": (ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),
+    "tvmc_commitment_device_tree": (ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),
+    "tvmc_commitment_auth_paths": (ctypes.c_int, [_vp, _szp, _sz, _u64p]),
+    "tvmc_commitment_auth_structure": (ctypes.c_int, [_vp, _szp, _sz, _u64p, _sz, _szp]),
+    "tvmc_auth_structure_indices": (ctypes.c_int, [_sz, _szp, _sz, _u64p, _sz, _szp]),
+    "tvmc_commitment_read_rows": (ctypes.c_int, [_vp, _szp, _sz, _u64p]),
+    "tvmc_commitment_read_columns": (ctypes.c_int, [_vp, _sz, _sz, _u64p]),
+    "tvmc_commitment_read_lde": (ctypes.c_int, [_vp, _u64p, ctypes.c_int]),
+    "tvmc_commitment_read_leaves": (ctypes.c_int, [_vp, _u64p]),
+    "tvmc_commitment_read_nodes": (ctypes.c_int, [_vp, _u64p]),
+    "tvmc_commitment_free": (ctypes.c_int, [_vp]),
+    "tvmc_commitment_phase_ms": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_float)]),
+    "tvmc_launch_count": (ctypes.c_ulonglong, []),
+    "tvmc_int_peak_probe": (ctypes.c_double, [_vp]),
+}
+
+_lib = None
+
+
+def lib():
+    """Load libtvmc.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(f"{LIB_PATH} is missing: build the CUDA extension first (make -C {HERE})")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(status: int) -> None:
+    if status == OK:
+        return
+    msg = lib().tvmc_last_error().decode(errors="replace")
+    if status == ERR_INVALID:
+        raise InvalidArgument(status, msg)
+    if status == ERR_RANGE:
+        raise OutOfRange(status, msg)
+    raise TvmcError(status, msg)
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(_u64p)
+
+
+def _u64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.uint64)
+
+
+# ---------------------------------------------------------------- host API
+
+def ntt(data, inverse: bool = False) -> np.ndarray:
+    """NTT::forward / NTT::inverse of each row of a (cols, n) array (or a 1-D array)."""
+    a = _u64(data).copy()
+    cols, n = (1, a.size) if a.ndim == 1 else a.shape
+    _check(lib().tvmc_ntt_host(_p(a), n, cols, int(inverse)))
+    return a
+
+
+def lde(trace_cm, expansion: int = 4, offset: int = 7) -> np.ndarray:
+    """LDE::extend_table on column-major (width, n) data -> (width, n*expansion)."""
+    t = _u64(trace_cm)
+    w, n = t.shape
+    out = np.empty((w, n * expansion), dtype=np.uint64)
+    _check(lib().tvmc_lde_host(_p(t), w, n, _p(out), n * expansion, offset))
+    return out
+
+
+def hash_varlen_rows(rows_rm) -> np.ndarray:
+    """Tip5::hash_varlen of every row of a row-major (rows, len) array -> (rows, 5)."""
+    t = _u64(rows_rm)
+    r, w = t.shape
+    out = np.zeros((r, 5), dtype=np.uint64)
+    _check(lib().tvmc_hash_varlen_host(_p(t) if t.size else _p(np.zeros(1, np.uint64)), r, w, _p(out)))
+    return out
+
+
+def hash_pairs(left, right) -> np.ndarray:
+    l, r = _u64(left).reshape(-1, 5), _u64(right).reshape(-1, 5)
+    out = np.zeros_like(l)
+    _check(lib().tvmc_hash_pairs_host(_p(l), _p(r), _p(out), l.shape[0]))
+    return out
+
+
+def tip5_permutations(states) -> np.ndarray:
+    s = _u64(states).reshape(-1, 16).copy()
+    _check(lib().tvmc_tip5_permutation_batch_host(_p(s), s.shape[0]))
+    return s
+
+
+def merkle_heap(leaves) -> np.ndarray:
+    lv = _u64(leaves).reshape(-1, 5)
+    n = lv.shape[0]
+    nodes = np.zeros((2 * n, 5), dtype=np.uint64)
+    _check(lib().tvmc_merkle_tree_heap_host(_p(lv), n, _p(nodes)))
+    return nodes
+
+
+def auth_structure_indices(num_leaves: int, leaves) -> np.ndarray:
+    """Heap indices of MerkleTree::authentication_structure, descending (host only)."""
+    ix = np.ascontiguousarray(leaves, dtype=np.uintp)
+    cap = max(1, ix.size * 64)
+    out = np.zeros(cap, dtype=np.uint64)
+    cnt = ctypes.c_size_t(0)
+    _check(lib().tvmc_auth_structure_indices(num_leaves, ix.ctypes.data_as(_szp), ix.size, _p(out), cap,
+                                             ctypes.byref(cnt)))
+    return out[: cnt.value]
+
+
+# ---------------------------------------------------------------- device API
+
+def _stream(stream) -> int | None:
+    if stream is None:
+        return None
+    return int(getattr(stream, "cuda_stream", stream))
+
+
+def ntt_gpu(d_data: int, n: int, cols: int, inverse: bool = False, stream=None) -> None:
+    f = lib().tvmc_ntt_inverse_batched_gpu if inverse else lib().tvmc_ntt_forward_batched_gpu
+    _check(f(d_data, n, cols, _stream(stream)))
+
+
+def lde_gpu(d_trace: int, cols: int, n: int, d_out: int, L: int, offset: int = 7, stream=None) -> None:
+    _check(lib().tvmc_lde_batch_gpu(d_trace, cols, n, d_out, L, 1, offset, _stream(stream)))
+
+
+def hash_rows_gpu(d_table: int, rows: int, cols: int, d_digests: int, stream=None) -> None:
+    _check(lib().tvmc_hash_bfield_rows_gpu(d_table, rows, cols, d_digests, _stream(stream)))
+
+
+def hash_xfield_rows_gpu(d_table: int, rows: int, xfe_cols: int, d_digests: int, stream=None) -> None:
+    _check(lib().tvmc_hash_xfield_rows_gpu(d_table, rows, xfe_cols, d_digests, _stream(stream)))
+
+
+def hash_pairs_gpu(d_left: int, d_right: int, d_out: int, count: int, stream=None) -> None:
+    _check(lib().tvmc_hash_pairs_gpu(d_left, d_right, d_out, count, _stream(stream)))
+
+
+def tip5_permutations_gpu(d_states: int, count: int, stream=None) -> None:
+    _check(lib().tvmc_tip5_permutation_batch_gpu(d_states, count, _stream(stream)))
+
+
+def merkle_tree_gpu(d_leaves: int, d_tree: int, n: int, stream=None) -> None:
+    _check(lib().tvmc_merkle_tree_gpu(d_leaves, d_tree, n, _stream(stream)))
+
+
+def merkle_root_gpu(d_leaves: int, d_root: int, n: int, stream=None) -> None:
+    _check(lib().tvmc_merkle_root_gpu(d_leaves, d_root, n, _stream(stream)))
+
+
+# ---------------------------------------------------------------- commitment
+
+class Commitment:
+    """A committed table: device-resident LDE (column-major) and heap tree.
+
+    Mirrors the reference's TableCommitment / MerkleTree accessors
+    (include/table/table_commitment.hpp, include/merkle/merkle_tree.hpp)."""
+
+    def __init__(self, trace, width: int | None = None, trace_len: int | None = None, expansion: int = 4,
+                 offset: int = 7, row_major: bool = False, device_ptr: bool = False, discard_lde: bool = False,
+                 stream=None, sync: bool = False, profile: bool = False):
+        flags = PROFILE if profile else 0
+        if device_ptr:
+            flags |= TRACE_DEVICE
+            ptr = int(trace)
+            self._keep = None
+            assert width is not None and trace_len is not None
+        else:
+            t = _u64(trace)
+            if row_major:
+                trace_len, width = t.shape
+            else:
+                width, trace_len = t.shape
+            self._keep = t  # the host buffer must live until the upload is done
+            ptr = t.ctypes.data if t.size else None
+        if row_major:
+            flags |= TRACE_ROW_MAJOR
+        if discard_lde:
+            flags |= DISCARD_LDE
+        if sync:
+            flags |= SYNC
+        h = _vp()
+        _check(lib().tvmc_commit(ptr, trace_len, width, expansion, offset, flags, _stream(stream), ctypes.byref(h)))
+        self.h = h
+        self.width = width
+        self.trace_len = trace_len
+        self.lde_len = trace_len * expansion
+
+    def _h(self):
+        if self.h is None:
+            raise ValueError("commitment already freed")
+        return self.h
+
+    def sync(self) -> None:
+        _check(lib().tvmc_commitment_sync(self._h()))
+        self._keep = None
+
+    def root(self) -> np.ndarray:
+        out = np.zeros(5, dtype=np.uint64)
+        _check(lib().tvmc_commitment_root(self._h(), _p(out)))
+        self._keep = None
+        return out
+
+    @property
+    def height(self) -> int:
+        return self.lde_len.bit_length() - 1
+
+    def auth_paths(self, leaves) -> np.ndarray:
+        ix = np.ascontiguousarray(leaves, dtype=np.uintp)
+        out = np.zeros((ix.size, self.height, 5), dtype=np.uint64)
+        _check(lib().tvmc_commitment_auth_paths(self._h(), ix.ctypes.data_as(_szp), ix.size,
+                                                _p(out) if out.size else None))
+        return out
+
+    def auth_structure(self, leaves) -> np.ndarray:
+        ix = np.ascontiguousarray(leaves, dtype=np.uintp)
+        cap = max(1, ix.size * max(1, self.height))
+        out = np.zeros((cap, 5), dtype=np.uint64)
+        cnt = ctypes.c_size_t(0)
+        _check(lib().tvmc_commitment_auth_structure(self._h(), ix.ctypes.data_as(_szp), ix.size, _p(out), cap,
+                                                    ctypes.byref(cnt)))
+        return out[: cnt.value]
+
+    def read_rows(self, rows) -> np.ndarray:
+        ix = np.ascontiguousarray(rows, dtype=np.uintp)
+        out = np.zeros((ix.size, self.width), dtype=np.uint64)
+        _check(lib().tvmc_commitment_read_rows(self._h(), ix.ctypes.data_as(_szp), ix.size,
+                                               _p(out) if out.size else None))
+        return out
+
+    def read_columns(self, col0: int, ncols: int) -> np.ndarray:
+        out = np.zeros((ncols, self.lde_len), dtype=np.uint64)
+        _check(lib().tvmc_commitment_read_columns(self._h(), col0, ncols, _p(out) if out.size else None))
+        return out
+
+    def lde(self, row_major: bool = False) -> np.ndarray:
+        shape = (self.lde_len, self.width) if row_major else (self.width, self.lde_len)
+        out = np.zeros(shape, dtype=np.uint64)
+        _check(lib().tvmc_commitment_read_lde(self._h(), _p(out) if out.size else None, int(row_major)))
+        return out
+
+    def leaves(self) -> np.ndarray:
+        out = np.zeros((self.lde_len, 5), dtype=np.uint64)
+        _check(lib().tvmc_commitment_read_leaves(self._h(), _p(out)))
+        return out
+
+    def nodes(self) -> np.ndarray:
+        out = np.zeros((2 * self.lde_len, 5), dtype=np.uint64)
+        _check(lib().tvmc_commitment_read_nodes(self._h(), _p(out)))
+        return out
+
+    def phase_ms(self) -> tuple[float, float, float]:
+        """(upload, LDE, row hash + tree) device milliseconds of a profiled commit."""
+        ms = (ctypes.c_float * 3)()
+        _check(lib().tvmc_commitment_phase_ms(self._h(), ms))
+        return ms[0], ms[1], ms[2]
+
+    def device_lde(self) -> int:
+        p = _vp()
+        _check(lib().tvmc_commitment_device_lde(self._h(), ctypes.byref(p)))
+        return p.value or 0
+
+    def device_tree(self) -> int:
+        p = _vp()
+        _check(lib().tvmc_commitment_device_tree(self._h(), ctypes.byref(p)))
+        return p.value or 0
+
+    def free(self) -> None:
+        if self.h is not None:
+            lib().tvmc_commitment_free(self.h)
+            self.h = None
+            self._keep = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.free()
