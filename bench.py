@@ -191,7 +191,7 @@ def run_reference(args):
             "warmup": args.warmup, "ms_per_step": 1e3 * cells / value, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64 (Goldilocks)", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": f"main 2^{args.log_n}x379 + aux 2^{args.log_n}x264 limbs, x4 LDE, Tip5 rows, "
+            "config": {"workload": f"main 2^{args.log_n}x{W_MAIN} + aux 2^{args.log_n}x{W_AUX} limbs, x4 LDE, Tip5 rows, "
                                    "Merkle", "trace_len": 1 << args.log_n, "widths": [W_MAIN, W_AUX],
                        "expansion": EXPANSION, "parallelism": "cpu"},
             "cpu_baseline": {"value": value, "unit": "cells/s", "cores": cores, "kind": "reference",
@@ -327,7 +327,7 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64 (Goldilocks)",
             "data": "synthetic uniform field elements",
-            "config": {"workload": f"main 2^{args.log_n}x379 + aux 2^{args.log_n}x264 limbs, x4 LDE (offset 7), "
+            "config": {"workload": f"main 2^{args.log_n}x{W_MAIN} + aux 2^{args.log_n}x{W_AUX} limbs, x4 LDE (offset 7), "
                                    "Tip5 row hash, Merkle (two trees)",
                        "trace_len": n, "lde_len": L, "widths": [W_MAIN, W_AUX], "expansion": EXPANSION,
                        "cells_per_step": cells_step, "l2": "inputs (5.4 GB) larger than L2",
@@ -362,7 +362,10 @@ def main():
     ap.add_argument("--log-n", type=int, default=LOG_N)
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--width-main", type=int, default=W_MAIN, help="main-table columns (profiling sizes)")
+    ap.add_argument("--width-aux", type=int, default=W_AUX, help="aux-table base limbs (profiling sizes)")
     args = ap.parse_args()
+    globals()["W_MAIN"], globals()["W_AUX"] = args.width_main, args.width_aux
     if args.impl == "reference":
         run_reference(args)
     else:

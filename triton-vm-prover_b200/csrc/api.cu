@@ -115,9 +115,9 @@ int get_plan(int logn, int le, uint64_t offset, LdePlan* pl) {
         T.pool_set = true;
     }
     if (!T.tw12_f) {
-        std::vector<uint64_t> f(2048), i(2048);
+        std::vector<uint64_t> f(4096), i(4096);
         uint64_t w = root_of_unity(12), wi = hinv(w), x = 1, y = 1;
-        for (int m = 0; m < 2048; m++) {
+        for (int m = 0; m < 4096; m++) {
             f[m] = x;
             i[m] = y;
             x = hmul(x, w);

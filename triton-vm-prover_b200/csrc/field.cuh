@@ -28,9 +28,54 @@ __device__ __forceinline__ uint64_t gl_reduce128(uint64_t lo, uint64_t hi) {
     return r;
 }
 
+// 64x64 -> 128-bit product as four 32-bit limbs (r3:r2:r1:r0), one carry
+// chain of 32-bit multiply-adds.
+__device__ __forceinline__ void gl_mul128(uint64_t a, uint64_t b, uint32_t& r0, uint32_t& r1, uint32_t& r2,
+                                          uint32_t& r3) {
+    const uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32), b0 = (uint32_t)b, b1 = (uint32_t)(b >> 32);
+    asm("{\n\t"
+        "mul.lo.u32 %0, %4, %6;\n\t"
+        "mul.hi.u32 %1, %4, %6;\n\t"
+        "mad.lo.cc.u32 %1, %4, %7, %1;\n\t"
+        "madc.hi.u32 %2, %4, %7, 0;\n\t"
+        "mad.lo.cc.u32 %1, %5, %6, %1;\n\t"
+        "madc.hi.cc.u32 %2, %5, %6, %2;\n\t"
+        "madc.hi.u32 %3, %5, %7, 0;\n\t"
+        "mad.lo.cc.u32 %2, %5, %7, %2;\n\t"
+        "addc.u32 %3, %3, 0;\n\t"
+        "}"
+        : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+        : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
+}
+
+// (r3:r2:r1:r0) -> (r1:r0) - r3 + r2*(2^32-1) (mod p) as a 64-bit representative.
+__device__ __forceinline__ uint64_t gl_reduce_limbs(uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3) {
+    uint32_t x0, x1, cm;
+    asm("{\n\t"
+        ".reg .u32 z, t0, t1, bm, u0, u1;\n\t"
+        "mov.u32 z, 0;\n\t"
+        "sub.cc.u32 t0, %3, %6;\n\t"    // t = (r1:r0) - r3
+        "subc.cc.u32 t1, %4, z;\n\t"
+        "subc.u32 bm, z, z;\n\t"        // borrow mask
+        "sub.cc.u32 t0, t0, bm;\n\t"    // borrow: t -= 2^32 - 1 (i.e. + p)
+        "subc.u32 t1, t1, z;\n\t"
+        "sub.cc.u32 u0, z, %5;\n\t"     // u = r2*(2^32 - 1) = (r2 << 32) - r2
+        "subc.u32 u1, %5, z;\n\t"
+        "add.cc.u32 %0, t0, u0;\n\t"    // x = t + u
+        "addc.cc.u32 %1, t1, u1;\n\t"
+        "addc.u32 %2, z, z;\n\t"        // carry out
+        "}"
+        : "=r"(x0), "=r"(x1), "=r"(cm)
+        : "r"(r0), "r"(r1), "r"(r2), "r"(r3));
+    const uint64_t x = ((uint64_t)x1 << 32) | x0;
+    return x + ((uint64_t)(0u - cm) & GL_EPS);  // carry: + (2^32 - 1); cannot wrap again
+}
+
 // a * b for any 64-bit representatives; partial result.
 __device__ __forceinline__ uint64_t gl_mul(uint64_t a, uint64_t b) {
-    return gl_reduce128(a * b, __umul64hi(a, b));
+    uint32_t r0, r1, r2, r3;
+    gl_mul128(a, b, r0, r1, r2, r3);
+    return gl_reduce_limbs(r0, r1, r2, r3);
 }
 __device__ __forceinline__ uint64_t gl_mul_c(uint64_t a, uint64_t b) { return gl_canon(gl_mul(a, b)); }
 

@@ -15,7 +15,7 @@
 
 namespace tvmc {
 
-constexpr int HASH_THREADS = 128;
+constexpr int HASH_THREADS = 256;
 constexpr int UP_THREADS = 128;
 
 __device__ __forceinline__ void store_digest(uint64_t* p, const uint64_t d[5]) {
@@ -43,7 +43,7 @@ __device__ __forceinline__ void subtree_levels(uint64_t* sd, uint64_t base, int 
     }
 }
 
-__global__ void __launch_bounds__(HASH_THREADS) k_hash_rows(
+__global__ void __launch_bounds__(HASH_THREADS, 2) k_hash_rows(
     const uint64_t* __restrict__ tab, uint64_t rstride, uint64_t cstride, uint64_t rows, uint32_t width,
     uint64_t* __restrict__ digests, uint64_t* __restrict__ tree, int layout, int fuse) {
     __shared__ uint32_t sbox[T5_SBOX_WORDS];

@@ -60,7 +60,7 @@ struct LdePlan {
     int logn;             // trace length N = 2^logn
     int log_exp;          // expansion E = 2^log_exp
     uint64_t offset;      // coset offset of the evaluation domain
-    const uint64_t* tw12_f;   // w_4096^m, m < 2048 (forward sub-DFT twiddles)
+    const uint64_t* tw12_f;   // w_4096^m, m < 4096 (forward sub-DFT twiddles)
     const uint64_t* tw12_i;   // inverse of the above
     const uint64_t* wn_f_lo;  // w_N^(e & 4095)
     const uint64_t* wn_f_hi;  // w_N^((e >> 12) * 4096)

@@ -7,13 +7,13 @@
 // given below.  The byte table is the offset Fermat cube map x -> (x+1)^3 - 1
 // over F_257, generated here rather than tabulated.
 //
-// B200 layout choices:
+// B200 layout choices (measured on sm_100a: 32-bit IMAD and DFMA are
+// half-rate, IMAD.HI quarter-rate, IMAD.WIDE takes two issue slots):
 //   * the byte table lives in shared memory as 64 words x 32 lanes, every lane
 //     owning its own bank, so the 8 lookups per word never conflict;
-//   * the MDS is computed exactly in integers: each word is split into 32-bit
-//     halves and the circulant products accumulate in 64-bit registers
-//     (coefficients < 2^16, sums < 2^52), then the two halves are recombined
-//     with one 128-bit reduction per output word.
+//   * the MDS runs exactly on the FP64 pipe (t5_mds), in parallel with the
+//     integer S-box work on the ALU/FMA pipes;
+//   * x^7 is a rolled loop over three groups of four words.
 #pragma once
 #include <cstdint>
 #include "field.cuh"
@@ -24,12 +24,9 @@ constexpr int T5_STATE = 16;
 constexpr int T5_RATE = 10;
 constexpr int T5_ROUNDS = 5;
 
-// Circulant MDS first column and round constants of Tip5 (published
-// parameters; identical to src/hash/tip5.cpp:27-79).
-__device__ __constant__ uint32_t c_t5_mds[T5_STATE] = {
-    61402, 1108, 28750, 33823, 7454, 43244, 53865, 12034,
-    56951, 27521, 41351, 40901, 12021, 59689, 26798, 17845};
-
+// Round constants of Tip5 (published parameters; identical to
+// src/hash/tip5.cpp:33-79).  The MDS first column (tip5.cpp:27-30) is inlined
+// in t5_mds below.
 __device__ __constant__ uint64_t c_t5_rc[T5_ROUNDS * T5_STATE] = {
     0xBD2A3DEB61AB60DEull, 0xEA7DF21AD9547ED2ull, 0x900B3677A1DE063Full, 0x1B46887E876C8677ull,
     0xD364D977889CFB97ull, 0xDC8DFAC843699F02ull, 0x375C405D7190DB58ull, 0x27924006D2B0D4B1ull,
@@ -105,30 +102,62 @@ __device__ __forceinline__ uint64_t t5_pow7(uint64_t x) {
     return gl_mul(x3, x4);
 }
 
+// Exact 32-bit <-> double conversions through the 2^52 exponent window.
+__device__ __forceinline__ double t5_u32_to_d(uint32_t v) {
+    return __hiloint2double(0x43300000, (int)v) - 4503599627370496.0;
+}
+__device__ __forceinline__ uint64_t t5_d_to_u52(double d) {
+    return (uint64_t)__double_as_longlong(d + 4503599627370496.0) & 0xFFFFFFFFFFFFFull;
+}
+
 // Circulant MDS: out[r] = sum_c M[(r - c) mod 16] * s[c] (mod p).
+// Each word is split into 32-bit halves; the two 16x16 circulant products run
+// as DFMAs on the FP64 pipe, exact because every partial sum is an integer
+// below 524757 * 2^32 < 2^52 (524757 = sum of the column).  The halves are then
+// recombined as lo + hi*2^32 with one 128-bit reduction per word.  Moving this
+// work off the integer pipes leaves them to the S-box arithmetic.
 __device__ __forceinline__ void t5_mds(uint64_t s[T5_STATE]) {
-    uint64_t lo[T5_STATE], hi[T5_STATE];
-#pragma unroll
-    for (int r = 0; r < T5_STATE; r++) { lo[r] = 0; hi[r] = 0; }
+    const double M[T5_STATE] = {61402, 1108, 28750, 33823, 7454, 43244, 53865, 12034,
+                                56951, 27521, 41351, 40901, 12021, 59689, 26798, 17845};
+    double dl[T5_STATE], dh[T5_STATE];
 #pragma unroll
     for (int c = 0; c < T5_STATE; c++) {
-        uint32_t l = (uint32_t)s[c], h = (uint32_t)(s[c] >> 32);
-#pragma unroll
-        for (int r = 0; r < T5_STATE; r++) {
-            uint32_t m = c_t5_mds[(r - c) & 15];
-            lo[r] += (uint64_t)m * l;
-            hi[r] += (uint64_t)m * h;
-        }
+        dl[c] = t5_u32_to_d((uint32_t)s[c]);
+        dh[c] = t5_u32_to_d((uint32_t)(s[c] >> 32));
     }
 #pragma unroll
     for (int r = 0; r < T5_STATE; r++) {
-        // value = lo + hi * 2^32 as a 128-bit number (sh:sl), sh < 2^21.
-        uint64_t sl = lo[r] + (hi[r] << 32);
-        uint64_t sh = (hi[r] >> 32) + (uint64_t)(sl < lo[r]);
-        uint64_t v = sh * GL_EPS;       // < 2^53
+        double al = 0.0, ah = 0.0;
+#pragma unroll
+        for (int c = 0; c < T5_STATE; c++) {
+            al = fma(M[(r - c) & 15], dl[c], al);
+            ah = fma(M[(r - c) & 15], dh[c], ah);
+        }
+        const uint64_t lo = t5_d_to_u52(al), hi = t5_d_to_u52(ah);
+        // lo + hi*2^32 as a 128-bit number (sh:sl) with sh < 2^21
+        const uint64_t sl = lo + (hi << 32);
+        const uint64_t sh = (hi >> 32) + (uint64_t)(sl < lo);
+        const uint64_t v = sh * GL_EPS;  // < 2^53
         uint64_t x = sl + v;
         if (x < v) x += GL_EPS;
         s[r] = x;
+    }
+}
+
+// x^7 on words 4..15 as three rolled groups of four (the words rotate by four
+// per group), which keeps the round body small enough for the instruction cache.
+__device__ __forceinline__ void t5_pow7_layer(uint64_t s[T5_STATE]) {
+#pragma unroll 1
+    for (int g = 0; g < 3; g++) {
+#pragma unroll
+        for (int i = 4; i < 8; i++) s[i] = t5_pow7(s[i]);
+        const uint64_t t0 = s[4], t1 = s[5], t2 = s[6], t3 = s[7];
+#pragma unroll
+        for (int i = 4; i < 12; i++) s[i] = s[i + 4];
+        s[12] = t0;
+        s[13] = t1;
+        s[14] = t2;
+        s[15] = t3;
     }
 }
 
@@ -137,8 +166,7 @@ __device__ __forceinline__ void t5_permutation(uint64_t s[T5_STATE], const uint3
     for (int rnd = 0; rnd < T5_ROUNDS; rnd++) {
 #pragma unroll
         for (int i = 0; i < 4; i++) s[i] = t5_split_lookup(s[i], lane_tbl);
-#pragma unroll
-        for (int i = 4; i < T5_STATE; i++) s[i] = t5_pow7(s[i]);
+        t5_pow7_layer(s);
         t5_mds(s);
 #pragma unroll
         for (int i = 0; i < T5_STATE; i++) s[i] = gl_add_pc(s[i], c_t5_rc[rnd * T5_STATE + i]);
