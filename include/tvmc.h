@@ -83,6 +83,25 @@ int tvmc_lde_batch_gpu(const uint64_t* d_traces, size_t num_columns, size_t trac
 int tvmc_lde_host(const uint64_t* traces, size_t num_columns, size_t trace_len, uint64_t* extended,
                   size_t extended_len, uint64_t extended_offset);
 
+/* Words (64 MiB) of the static device array used by tvmc_lde_batch_noalloc_gpu. */
+#define TVMC_NOALLOC_SCRATCH_WORDS ((size_t)1 << 23)
+/* The same LDE as tvmc_lde_batch_gpu, same arguments and results, but it never
+ * allocates device memory: intermediates and twiddle tables live in one static
+ * device array of TVMC_NOALLOC_SCRATCH_WORDS words that every GPU loading this
+ * library keeps until the process exits.  For callers that may not call the
+ * CUDA allocator (a prover running under a pre-reserved or custom memory
+ * manager, or a latency-critical loop where cudaMalloc's implicit
+ * synchronisation is not acceptable).  Limit: trace_len * (1 + expansion)
+ * must fit in the array minus its 100352 table words (e.g. 2^20 rows at
+ * expansion 4); larger sizes return TVMC_ERR_UNSUPPORTED.  The first call on
+ * a device looks up the array's device address (cudaGetSymbolAddress), so
+ * make that first call before capturing any stream.  All calls share the
+ * array: calls that overlap on the GPU race, so issue them on one stream.
+ * No counterpart in the reference. */
+int tvmc_lde_batch_noalloc_gpu(const uint64_t* d_traces, size_t num_columns, size_t trace_len,
+                               uint64_t* d_extended, size_t extended_len, uint64_t trace_offset,
+                               uint64_t extended_offset, void* stream);
+
 /* ---- Tip5 (include/gpu/kernels/row_hash_kernel.cuh:26-49, src/hash/tip5.cpp) ---- */
 
 /* Tip5::hash_varlen of every row of a column-major table (d_table[col*num_rows + row]).

@@ -337,6 +337,11 @@ int auth_structure_nodes(size_t n, const size_t* leaf_idx, size_t count, std::ve
 
 }  // namespace
 
+int tvmc::set_error(int code, const char* msg) {
+    g_err = msg;
+    return code;
+}
+
 struct tvmc_commitment {
     int device = 0;
     cudaStream_t stream = nullptr;

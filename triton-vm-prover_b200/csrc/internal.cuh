@@ -8,6 +8,8 @@ namespace tvmc {
 
 // Number of kernels this library has launched (all devices, all threads).
 void count_launch();
+// Records `msg` as the calling thread's tvmc_last_error() text; returns code.
+int set_error(int code, const char* msg);
 
 // Merkle node storage layouts.
 //   HEAP: 2n digests, node h at h (root 1, leaves [n, 2n), slot 0 unused) --

@@ -61,6 +61,8 @@ SIGNATURES = {
     "tvmc_ntt_host": (ctypes.c_int, [_u64p, _sz, _sz, ctypes.c_int]),
     "tvmc_lde_batch_gpu": (ctypes.c_int, [_vp, _sz, _sz, _vp, _sz, ctypes.c_uint64, ctypes.c_uint64, _vp]),
     "tvmc_lde_host": (ctypes.c_int, [_u64p, _sz, _sz, _u64p, _sz, ctypes.c_uint64]),
+    "tvmc_lde_batch_noalloc_gpu": (ctypes.c_int, [_vp, _sz, _sz, _vp, _sz, ctypes.c_uint64, ctypes.c_uint64,
+                                                  _vp]),
     "tvmc_hash_bfield_rows_gpu": (ctypes.c_int, [_vp, _sz, _sz, _vp, _vp]),
     "tvmc_hash_xfield_rows_gpu": (ctypes.c_int, [_vp, _sz, _sz, _vp, _vp]),
     "tvmc_hash_varlen_host": (ctypes.c_int, [_u64p, _sz, _sz, _u64p]),
