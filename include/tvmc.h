@@ -144,6 +144,18 @@ typedef struct tvmc_commitment tvmc_commitment;
 #define TVMC_DISCARD_LDE 0x4u     /* free the LDE after hashing; keep only the tree */
 #define TVMC_SYNC 0x8u            /* return only when the commitment is complete */
 #define TVMC_PROFILE 0x10u        /* record CUDA events around the upload, LDE and hash/tree phases */
+#define TVMC_FRUGAL 0x20u         /* streaming mode: LDE in 10-column-aligned stripes absorbed into
+                                     resident sponge states; the full LDE is never stored (implies
+                                     TVMC_DISCARD_LDE); for very tall tables (2^22 rows and up) */
+
+/* Tuning knobs (process-wide; 0 restores the default):
+ *   "frugal_stripe_cols"  columns per TVMC_FRUGAL stripe, rounded down to a multiple of 10
+ *                         (default: the widest stripe whose LDE fits in 2 GiB, at least 10)
+ *   "lde_scratch_bytes"   LDE intermediate budget per call (default 2 GiB); columns are
+ *                         processed in chunks that fit
+ * Unknown keys return TVMC_ERR_INVALID. */
+int tvmc_set_tuning(const char* key, long long value);
+int tvmc_get_tuning(const char* key, long long* value);
 
 /* Commit to one table: LDE of every column onto offset * <w_{trace_len*expansion}>
  * (expansion a power of two <= 16), Tip5 hash_varlen of every LDE row, Merkle
@@ -184,6 +196,32 @@ int tvmc_commitment_read_lde(tvmc_commitment* c, uint64_t* out, int row_major);
 int tvmc_commitment_read_leaves(tvmc_commitment* c, uint64_t* out);
 int tvmc_commitment_read_nodes(tvmc_commitment* c, uint64_t* out);
 int tvmc_commitment_free(tvmc_commitment* c);
+/* ---- batched commitment of many tables (one CUDA-graph launch per run) ---- */
+
+typedef struct tvmc_batch tvmc_batch;
+typedef struct {
+    size_t trace_len;   /* power of two, <= 2^22 */
+    size_t width;       /* base columns (3 per XFieldElement column) */
+    uint32_t expansion; /* power of two <= 16 */
+    uint64_t offset;    /* coset offset of the evaluation domain */
+} tvmc_table_shape;
+
+/* Plan a batch of `count` tables of uneven heights and widths: allocate every
+ * table's input buffer, LDE, tree and scratch once, and capture the whole
+ * commitment of all tables (LDE -> row hash -> Merkle, tables spread over
+ * worker streams that overlap on the device) into one instantiated CUDA
+ * graph.  Worker-stream count: tuning knob "batch_streams" (default 8). */
+int tvmc_batch_create(const tvmc_table_shape* shapes, size_t count, tvmc_batch** out);
+/* Device input buffer of table i: column-major [width][trace_len]; fill it
+ * (e.g. cudaMemcpyAsync on the run stream) before tvmc_batch_run. */
+int tvmc_batch_input(tvmc_batch* b, size_t i, uint64_t** d_trace);
+/* Commit every table: one cudaGraphLaunch on `stream`. */
+int tvmc_batch_run(tvmc_batch* b, void* stream);
+/* Commitment handle of table i (valid until tvmc_batch_free; do not free it):
+ * all tvmc_commitment_* accessors work on it and wait for the last run. */
+int tvmc_batch_commitment(tvmc_batch* b, size_t i, tvmc_commitment** c);
+int tvmc_batch_free(tvmc_batch* b);
+
 /* For a TVMC_PROFILE commitment: device milliseconds of [upload (or transpose),
  * LDE, row hash + Merkle tree]; with a pipelined host upload the upload is
  * counted inside the LDE phase. */

@@ -62,3 +62,20 @@ def from_dev(t):
 def dev_empty(*shape):
     import torch
     return torch.empty(*shape, dtype=torch.int64, device="cuda")
+
+
+def _cudart():
+    """The CUDA runtime libtvmc.so itself links (loaded with it)."""
+    import ctypes
+    import tvmc
+    tvmc.lib()
+    rt = ctypes.CDLL("libcudart.so.12")
+    rt.cudaMemcpy.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]
+    return rt
+
+
+def memcpy_h2d(dst_ptr, host):
+    """Synchronous host -> device copy into a raw device pointer."""
+    host = np.ascontiguousarray(host)
+    rc = _cudart().cudaMemcpy(dst_ptr, host.ctypes.data, host.nbytes, 1)  # cudaMemcpyHostToDevice
+    assert rc == 0, rc

@@ -187,11 +187,20 @@ int get_plan(int logn, int le, uint64_t offset, LdePlan* pl) {
 
 cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
-// Column chunk so that LDE scratch stays under ~2 GiB.
+// Process-wide tuning knobs (tvmc_set_tuning); 0 = default.
+std::atomic<long long> g_tune_stripe_cols{0};
+std::atomic<long long> g_tune_scratch_bytes{0};
+
+size_t scratch_budget() {
+    const long long b = g_tune_scratch_bytes.load();
+    return b > 0 ? (size_t)b : (size_t(2) << 30);
+}
+
+// Column chunk so that LDE scratch stays within the budget.
 size_t lde_chunk_cols(int logn, int le, size_t width) {
     size_t per = lde_scratch_words(logn, le, 1) * 8;
     if (per == 0) return width ? width : 1;
-    size_t lim = (size_t(2) << 30) / per;
+    size_t lim = scratch_budget() / per;
     if (lim < 1) lim = 1;
     return std::min(width ? width : size_t(1), lim);
 }
@@ -237,7 +246,7 @@ int copy_stream(cudaStream_t* out) {
 // chunk k.  Returns after enqueueing; `st` is ordered after every copy.
 int upload_lde_pipelined(const LdePlan& pl, const uint64_t* h_trace, size_t n, size_t width, uint64_t* d_out,
                          size_t L, cudaStream_t st) {
-    cudaStream_t cs;
+    cudaStream_t cs = nullptr;
     int rc = copy_stream(&cs);
     if (rc) return rc;
     size_t chunk = lde_chunk_cols(pl.logn, pl.log_exp, width);
@@ -315,6 +324,58 @@ struct DBuf {
     cudaError_t alloc(size_t words) { return cudaMalloc((void**)&p, words ? words * 8 : 8); }
 };
 
+// TVMC_FRUGAL commit: the LDE is produced stripe by stripe (10-column aligned)
+// and each stripe is absorbed at once into the per-row sponge capacity state,
+// so only one stripe of LDE (plus 48 bytes of state per row) is ever resident.
+// Leaves go straight into the heap tree `nodes`, which the last stripe completes.
+int commit_frugal(const LdePlan& pl, const uint64_t* trace, bool dev, bool rm, size_t n, size_t width, size_t L,
+                  uint64_t* nodes, cudaStream_t st, cudaEvent_t* prof) {
+    const size_t NW = n * width;
+    const uint64_t* src = trace;
+    uint64_t *up = nullptr, *cm = nullptr, *cap = nullptr, *stripe = nullptr, *scratch = nullptr;
+    cudaError_t e = cudaSuccess;
+    if (width && !dev) {
+        e = cudaMallocAsync((void**)&up, NW * 8, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(up, trace, NW * 8, cudaMemcpyHostToDevice, st);
+        src = up;
+    }
+    if (e == cudaSuccess && width && rm) {
+        e = cudaMallocAsync((void**)&cm, NW * 8, st);
+        if (e == cudaSuccess) e = launch_transpose(src, width, cm, n, n, width, st);
+        src = cm;
+    }
+    if (prof) cudaEventRecord(prof[1], st);
+    // stripe width: a multiple of 10 columns whose LDE fits the knob or 2 GiB
+    size_t sc = g_tune_stripe_cols.load() > 0 ? (size_t)g_tune_stripe_cols.load()
+                                                : ((size_t(2) << 30) / (L * 8)) / 10 * 10;
+    sc = std::max<size_t>(10, sc / 10 * 10);
+    const size_t stripe_cols = std::min(sc, std::max<size_t>(width, 1));
+    const size_t chunk = std::min(lde_chunk_cols(pl.logn, pl.log_exp, stripe_cols), stripe_cols);
+    const size_t sw = lde_scratch_words(pl.logn, pl.log_exp, chunk);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&cap, 6 * L * 8, st);
+    if (e == cudaSuccess && width) e = cudaMallocAsync((void**)&stripe, stripe_cols * L * 8, st);
+    if (e == cudaSuccess && sw) e = cudaMallocAsync((void**)&scratch, sw * 8, st);
+    size_t c0 = 0;
+    bool first = true;
+    while (e == cudaSuccess) {
+        const size_t nc = std::min(sc, width - c0);
+        const bool last = c0 + nc == width;
+        for (size_t k = 0; k < nc && e == cudaSuccess; k += chunk) {
+            const size_t kc = std::min(chunk, nc - k);
+            e = launch_lde(pl, src + (c0 + k) * n, n, stripe + k * L, L, kc, scratch, st);
+        }
+        if (e == cudaSuccess) e = launch_absorb_stripe(stripe, L, (uint32_t)nc, cap, first, last, nodes, st);
+        first = false;
+        c0 += nc;
+        if (last) break;
+    }
+    for (uint64_t* p : {up, cm, cap, stripe, scratch})
+        if (p) cudaFreeAsync(p, st);
+    if (prof) cudaEventRecord(prof[2], st);
+    if (e != cudaSuccess) return cuda_fail(e, "frugal commit");
+    return TVMC_OK;
+}
+
 // Needed-minus-computable node set of a batch of leaf paths, descending.
 int auth_structure_nodes(size_t n, const size_t* leaf_idx, size_t count, std::vector<uint64_t>* res) {
     std::vector<uint64_t> path, need;
@@ -351,6 +412,38 @@ struct tvmc_commitment {
     cudaEvent_t done = nullptr;
     // TVMC_PROFILE: events at start / after upload / after LDE / after hash+tree
     cudaEvent_t prof[4] = {nullptr, nullptr, nullptr, nullptr};
+    bool batch_owned = false;  // freed by tvmc_batch_free only
+};
+
+namespace {
+void destroy_commitment(tvmc_commitment* c) {
+    if (c->done) {
+        cudaEventSynchronize(c->done);
+        cudaEventDestroy(c->done);
+    } else {
+        cudaStreamSynchronize(c->stream);
+    }
+    for (auto ev : c->prof)
+        if (ev) cudaEventDestroy(ev);
+    if (c->d_lde) cudaFree(c->d_lde);
+    if (c->d_nodes) cudaFree(c->d_nodes);
+    delete c;
+}
+std::atomic<long long> g_tune_batch_streams{0};
+}  // namespace
+
+struct tvmc_batch {
+    int device = 0;
+    std::vector<tvmc_table_shape> shapes;
+    std::vector<tvmc_commitment*> tables;  // batch-owned handles (LDE + tree)
+    std::vector<uint64_t*> inputs;         // per-table device trace buffers
+    std::vector<uint64_t*> scratch;        // per-worker LDE scratch
+    std::vector<cudaStream_t> workers;
+    std::vector<cudaEvent_t> events;       // fork + one join per worker
+    cudaStream_t capture = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    unsigned long long kernels_per_run = 0;
 };
 
 extern "C" {
@@ -373,6 +466,25 @@ const char* tvmc_status_string(int s) {
 int tvmc_version(void) { return 1; }
 
 unsigned long long tvmc_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
+int tvmc_set_tuning(const char* key, long long value) {
+    if (!key) return fail(TVMC_ERR_INVALID, "null tuning key");
+    if (value < 0) return fail(TVMC_ERR_INVALID, "tuning value must be >= 0");
+    if (!strcmp(key, "frugal_stripe_cols")) g_tune_stripe_cols = value;
+    else if (!strcmp(key, "lde_scratch_bytes")) g_tune_scratch_bytes = value;
+    else if (!strcmp(key, "batch_streams")) g_tune_batch_streams = value;
+    else return fail(TVMC_ERR_INVALID, "unknown tuning key '%s'", key);
+    return TVMC_OK;
+}
+
+int tvmc_get_tuning(const char* key, long long* value) {
+    if (!key || !value) return fail(TVMC_ERR_INVALID, "null argument");
+    if (!strcmp(key, "frugal_stripe_cols")) *value = g_tune_stripe_cols;
+    else if (!strcmp(key, "lde_scratch_bytes")) *value = g_tune_scratch_bytes;
+    else if (!strcmp(key, "batch_streams")) *value = g_tune_batch_streams;
+    else return fail(TVMC_ERR_INVALID, "unknown tuning key '%s'", key);
+    return TVMC_OK;
+}
 
 int tvmc_device_count(void) {
     int n = 0;
@@ -536,7 +648,8 @@ int tvmc_commit(const uint64_t* trace, size_t trace_len, size_t width, uint32_t 
     *out = nullptr;
     if (!is_pow2(expansion) || expansion > 16)
         return fail(TVMC_ERR_INVALID, "expansion factor %u is not a power of 2 <= 16", expansion);
-    if (flags & ~(TVMC_TRACE_DEVICE | TVMC_TRACE_ROW_MAJOR | TVMC_DISCARD_LDE | TVMC_SYNC | TVMC_PROFILE))
+    if (flags & ~(TVMC_TRACE_DEVICE | TVMC_TRACE_ROW_MAJOR | TVMC_DISCARD_LDE | TVMC_SYNC | TVMC_PROFILE |
+                  TVMC_FRUGAL))
         return fail(TVMC_ERR_INVALID, "unknown flag bits 0x%x", flags);
     int logn, le;
     int rc = check_lde_sizes(trace_len, trace_len * expansion, &logn, &le);
@@ -557,8 +670,9 @@ int tvmc_commit(const uint64_t* trace, size_t trace_len, size_t width, uint32_t 
         return code;
     };
     const size_t NW = trace_len * width;
+    const bool frugal = flags & TVMC_FRUGAL;
     if (cudaMalloc((void**)&c->d_nodes, 2 * c->L * 40) != cudaSuccess ||
-        (width && cudaMalloc((void**)&c->d_lde, c->L * width * 8) != cudaSuccess)) {
+        (width && !frugal && cudaMalloc((void**)&c->d_lde, c->L * width * 8) != cudaSuccess)) {
         cudaGetLastError();
         return bail(fail(TVMC_ERR_NOMEM, "cannot allocate LDE (%zu x %zu) and tree", c->L, width));
     }
@@ -571,7 +685,10 @@ int tvmc_commit(const uint64_t* trace, size_t trace_len, size_t width, uint32_t 
         cudaEventRecord(c->prof[0], st);
     }
     const bool dev = flags & TVMC_TRACE_DEVICE, rm = flags & TVMC_TRACE_ROW_MAJOR;
-    if (width && !dev && !rm) {
+    if (frugal) {
+        rc = commit_frugal(pl, trace, dev, rm, trace_len, width, c->L, c->d_nodes, st, prof ? c->prof : nullptr);
+        if (rc) return bail(rc);
+    } else if (width && !dev && !rm) {
         // host column-major trace: upload column chunks on a copy stream,
         // overlapping the LDE of the previous chunk
         if (prof) cudaEventRecord(c->prof[1], st);
@@ -605,9 +722,12 @@ int tvmc_commit(const uint64_t* trace, size_t trace_len, size_t width, uint32_t 
     } else if (prof) {
         cudaEventRecord(c->prof[1], st);
     }
-    if (prof) cudaEventRecord(c->prof[2], st);
-    cudaError_t e = launch_hash_rows(c->d_lde, 1, c->L, c->L, (uint32_t)width, nullptr, c->d_nodes, LAYOUT_HEAP, st);
-    if (e != cudaSuccess) return bail(cuda_fail(e, "hash/merkle"));
+    if (prof && !frugal) cudaEventRecord(c->prof[2], st);
+    if (!frugal) {  // (the frugal stripes already hashed every row and built the tree)
+        cudaError_t e =
+            launch_hash_rows(c->d_lde, 1, c->L, c->L, (uint32_t)width, nullptr, c->d_nodes, LAYOUT_HEAP, st);
+        if (e != cudaSuccess) return bail(cuda_fail(e, "hash/merkle"));
+    }
     if (prof) cudaEventRecord(c->prof[3], st);
     if ((flags & TVMC_DISCARD_LDE) && c->d_lde) {
         cudaFreeAsync(c->d_lde, st);  // stream-ordered after the hash kernel
@@ -765,17 +885,161 @@ int tvmc_commitment_read_nodes(tvmc_commitment* c, uint64_t* out) {
 
 int tvmc_commitment_free(tvmc_commitment* c) {
     if (!c) return TVMC_OK;
-    if (c->done) {
-        cudaEventSynchronize(c->done);
-        cudaEventDestroy(c->done);
-    } else if (c->stream || true) {
-        cudaStreamSynchronize(c->stream);
+    if (c->batch_owned) return fail(TVMC_ERR_INVALID, "commitment belongs to a batch; free the batch");
+    destroy_commitment(c);
+    return TVMC_OK;
+}
+
+int tvmc_batch_free(tvmc_batch* b) {
+    if (!b) return TVMC_OK;
+    for (auto* c : b->tables) destroy_commitment(c);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    for (auto s : b->workers) cudaStreamDestroy(s);
+    if (b->capture) cudaStreamDestroy(b->capture);
+    for (auto e : b->events) cudaEventDestroy(e);
+    for (auto p : b->inputs) cudaFree(p);
+    for (auto p : b->scratch) cudaFree(p);
+    delete b;
+    return TVMC_OK;
+}
+
+int tvmc_batch_create(const tvmc_table_shape* shapes, size_t count, tvmc_batch** out) {
+    if (!out || (count && !shapes)) return fail(TVMC_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (count == 0) return fail(TVMC_ERR_INVALID, "empty batch");
+    std::vector<LdePlan> plans(count);
+    for (size_t i = 0; i < count; i++) {
+        const tvmc_table_shape& s = shapes[i];
+        if (!is_pow2(s.expansion) || s.expansion > 16)
+            return fail(TVMC_ERR_INVALID, "table %zu: expansion %u is not a power of 2 <= 16", i, s.expansion);
+        int logn, le;
+        int rc = check_lde_sizes(s.trace_len, s.trace_len * s.expansion, &logn, &le);
+        if (rc) return rc;
+        if ((rc = get_plan(logn, le, s.offset, &plans[i]))) return rc;  // tables built before capture
     }
-    for (auto ev : c->prof)
-        if (ev) cudaEventDestroy(ev);
-    if (c->d_lde) cudaFree(c->d_lde);
-    if (c->d_nodes) cudaFree(c->d_nodes);
-    delete c;
+    tvmc_batch* b = new tvmc_batch();
+    auto bail = [&](int code) {
+        tvmc_batch_free(b);
+        return code;
+    };
+    CK(cudaGetDevice(&b->device));
+    b->shapes.assign(shapes, shapes + count);
+    const long long ks = g_tune_batch_streams.load();
+    const size_t K = std::min<size_t>(count, ks > 0 ? (size_t)ks : 8);
+    // tables, largest first, onto the least-loaded worker
+    std::vector<size_t> order(count);
+    for (size_t i = 0; i < count; i++) order[i] = i;
+    auto work = [&](size_t i) { return (double)shapes[i].trace_len * shapes[i].expansion * (shapes[i].width + 1); };
+    std::sort(order.begin(), order.end(), [&](size_t a, size_t c) { return work(a) > work(c); });
+    std::vector<std::vector<size_t>> assign(K);
+    std::vector<double> load(K, 0.0);
+    for (size_t i : order) {
+        const size_t w = std::min_element(load.begin(), load.end()) - load.begin();
+        assign[w].push_back(i);
+        load[w] += work(i);
+    }
+    // buffers
+    const size_t budget = std::max<size_t>(scratch_budget() / K, size_t(64) << 20);
+    std::vector<size_t> chunk(count);
+    for (size_t i = 0; i < count; i++) {
+        const tvmc_table_shape& s = shapes[i];
+        tvmc_commitment* c = new tvmc_commitment();
+        c->batch_owned = true;
+        c->device = b->device;
+        c->n = s.trace_len;
+        c->width = s.width;
+        c->L = s.trace_len * s.expansion;
+        b->tables.push_back(c);
+        uint64_t* in = nullptr;
+        if (cudaMalloc((void**)&c->d_nodes, 2 * c->L * 40) != cudaSuccess ||
+            (s.width && cudaMalloc((void**)&c->d_lde, c->L * s.width * 8) != cudaSuccess) ||
+            (s.width && cudaMalloc((void**)&in, s.trace_len * s.width * 8) != cudaSuccess)) {
+            cudaGetLastError();
+            if (in) cudaFree(in);
+            return bail(fail(TVMC_ERR_NOMEM, "cannot allocate table %zu of the batch", i));
+        }
+        b->inputs.push_back(in);
+        CK(cudaEventCreateWithFlags(&c->done, cudaEventDisableTiming));
+        const size_t per = lde_scratch_words(plans[i].logn, plans[i].log_exp, 1) * 8;
+        chunk[i] = per ? std::max<size_t>(1, std::min(s.width, budget / per)) : std::max<size_t>(s.width, 1);
+    }
+    for (size_t w = 0; w < K; w++) {
+        size_t words = 0;
+        for (size_t i : assign[w]) words = std::max(words, lde_scratch_words(plans[i].logn, plans[i].log_exp, chunk[i]));
+        uint64_t* p = nullptr;
+        if (words && cudaMalloc((void**)&p, words * 8) != cudaSuccess) {
+            cudaGetLastError();
+            return bail(fail(TVMC_ERR_NOMEM, "cannot allocate batch scratch"));
+        }
+        b->scratch.push_back(p);
+        cudaStream_t s;
+        CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        b->workers.push_back(s);
+    }
+    for (size_t e = 0; e <= K; e++) {
+        cudaEvent_t ev;
+        CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        b->events.push_back(ev);
+    }
+    CK(cudaStreamCreateWithFlags(&b->capture, cudaStreamNonBlocking));
+    // capture: fork -> per-worker table commits -> join
+    const unsigned long long k0 = g_launches.load();
+    CK(cudaStreamBeginCapture(b->capture, cudaStreamCaptureModeRelaxed));
+    cudaError_t e = cudaEventRecord(b->events[0], b->capture);
+    for (size_t w = 0; w < K && e == cudaSuccess; w++) {
+        cudaStream_t st = b->workers[w];
+        e = cudaStreamWaitEvent(st, b->events[0], 0);
+        for (size_t t = 0; t < assign[w].size() && e == cudaSuccess; t++) {
+            const size_t i = assign[w][t];
+            tvmc_commitment* c = b->tables[i];
+            const size_t W = shapes[i].width, N = shapes[i].trace_len;
+            e = cudaMemsetAsync(c->d_nodes, 0, 40, st);
+            for (size_t c0 = 0; c0 < W && e == cudaSuccess; c0 += chunk[i]) {
+                const size_t nc = std::min(chunk[i], W - c0);
+                e = launch_lde(plans[i], b->inputs[i] + c0 * N, N, c->d_lde + c0 * c->L, c->L, nc, b->scratch[w], st);
+            }
+            if (e == cudaSuccess)
+                e = launch_hash_rows(c->d_lde, 1, c->L, c->L, (uint32_t)W, nullptr, c->d_nodes, LAYOUT_HEAP, st);
+        }
+        if (e == cudaSuccess) e = cudaEventRecord(b->events[w + 1], st);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(b->capture, b->events[w + 1], 0);
+    }
+    cudaGraph_t g = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(b->capture, &g);
+    b->graph = g;
+    b->kernels_per_run = g_launches.load() - k0;
+    g_launches.fetch_sub(b->kernels_per_run);  // counted again at every run
+    if (e != cudaSuccess) return bail(cuda_fail(e, "batch capture"));
+    if (e2 != cudaSuccess) return bail(cuda_fail(e2, "batch capture end"));
+    CK(cudaGraphInstantiate(&b->exec, b->graph, 0));
+    *out = b;
+    return TVMC_OK;
+}
+
+int tvmc_batch_input(tvmc_batch* b, size_t i, uint64_t** d_trace) {
+    if (!b || !d_trace) return fail(TVMC_ERR_INVALID, "null argument");
+    if (i >= b->tables.size()) return fail(TVMC_ERR_RANGE, "table %zu out of range", i);
+    *d_trace = b->inputs[i];
+    return TVMC_OK;
+}
+
+int tvmc_batch_run(tvmc_batch* b, void* stream) {
+    if (!b) return fail(TVMC_ERR_INVALID, "null batch");
+    cudaStream_t st = as_stream(stream);
+    CK(cudaGraphLaunch(b->exec, st));
+    g_launches.fetch_add(b->kernels_per_run);
+    for (auto* c : b->tables) {
+        c->stream = st;
+        CK(cudaEventRecord(c->done, st));
+    }
+    return TVMC_OK;
+}
+
+int tvmc_batch_commitment(tvmc_batch* b, size_t i, tvmc_commitment** c) {
+    if (!b || !c) return fail(TVMC_ERR_INVALID, "null argument");
+    if (i >= b->tables.size()) return fail(TVMC_ERR_RANGE, "table %zu out of range", i);
+    *c = b->tables[i];
     return TVMC_OK;
 }
 

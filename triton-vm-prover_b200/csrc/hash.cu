@@ -101,6 +101,64 @@ __global__ void __launch_bounds__(HASH_THREADS, 2) k_hash_rows(
     }
 }
 
+// Frugal streaming: absorb one stripe of `ncols` LDE columns (column-major,
+// stride L) into the sponge of every row.  Between stripes only the capacity
+// words 10..15 survive (overwrite mode replaces the rate at every absorb), so
+// they are all that is stored: cap[w*L + r], w < 6 (coalesced per word).  The
+// first stripe starts from the zero state.  Every stripe but the last must
+// hold whole 10-column chunks; the last one appends the hash_varlen padding
+// (rest, 1, zeros), finishes the digest and writes it as tree leaf n + r,
+// building the lowest log2(blockDim) levels in shared memory as k_hash_rows does.
+__global__ void __launch_bounds__(HASH_THREADS, 2) k_absorb_stripe(
+    const uint64_t* __restrict__ stripe, uint64_t L, uint32_t ncols, uint64_t* __restrict__ cap, int first,
+    int last, uint64_t* __restrict__ tree, int fuse) {
+    __shared__ uint32_t sbox[T5_SBOX_WORDS];
+    __shared__ uint64_t sd[HASH_THREADS * 5];
+    t5_sbox_init(sbox);
+    __syncthreads();
+    const uint32_t* lt = sbox + (threadIdx.x & 31);
+    const uint64_t row = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;  // L is a multiple of blockDim
+    const uint64_t* p = stripe + row;
+
+    uint64_t s[T5_STATE];
+#pragma unroll
+    for (int i = 0; i < T5_RATE; i++) s[i] = 0;
+#pragma unroll
+    for (int i = 0; i < T5_STATE - T5_RATE; i++) s[T5_RATE + i] = first ? 0 : cap[(uint64_t)i * L + row];
+
+    const uint32_t full = ncols / T5_RATE;
+    const uint32_t rem = ncols - full * T5_RATE;
+    uint64_t nx[T5_RATE];
+#pragma unroll
+    for (int i = 0; i < T5_RATE; i++) nx[i] = (full > 0 || (uint32_t)i < rem) ? __ldg(p + (uint64_t)i * L) : 0;
+    for (uint32_t k = 0; k < full; k++) {
+#pragma unroll
+        for (int i = 0; i < T5_RATE; i++) s[i] = nx[i];
+        const uint32_t c0 = (k + 1) * T5_RATE;
+        const uint32_t lim = (k + 1 < full) ? T5_RATE : rem;
+#pragma unroll
+        for (int i = 0; i < T5_RATE; i++) nx[i] = ((uint32_t)i < lim) ? __ldg(p + (uint64_t)(c0 + i) * L) : 0;
+        t5_permutation(s, lt);
+    }
+    if (!last) {
+#pragma unroll
+        for (int i = 0; i < T5_STATE - T5_RATE; i++) cap[(uint64_t)i * L + row] = s[T5_RATE + i];
+        return;
+    }
+#pragma unroll
+    for (int i = 0; i < T5_RATE; i++) s[i] = ((uint32_t)i < rem) ? nx[i] : ((uint32_t)i == rem ? 1 : 0);
+    t5_permutation(s, lt);
+    uint64_t d[5];
+#pragma unroll
+    for (int i = 0; i < 5; i++) d[i] = gl_canon(s[i]);
+    store_digest(tree + 5 * (L + row), d);
+    if (fuse > 0) {
+        store_digest(sd + 5 * threadIdx.x, d);
+        __syncthreads();
+        subtree_levels(sd, L + (uint64_t)blockIdx.x * blockDim.x, fuse, tree, L, LAYOUT_HEAP, lt);
+    }
+}
+
 // One launch builds up to `levels` levels above the level of m nodes.
 __global__ void __launch_bounds__(UP_THREADS) k_merkle_up(uint64_t* __restrict__ tree, uint64_t n,
                                                           uint64_t m, int layout, int levels) {
@@ -294,6 +352,27 @@ cudaError_t launch_gather_rows(const uint64_t* table, uint64_t ld, uint32_t widt
     count_launch();
     k_gather_rows<<<grid_for(count * width, 256), 256, 0, st>>>(table, ld, width, rows, count, out);
     return cudaGetLastError();
+}
+
+cudaError_t launch_absorb_stripe(const uint64_t* stripe, uint64_t L, uint32_t ncols, uint64_t* cap, int first,
+                                 int last, uint64_t* tree, cudaStream_t st) {
+    const unsigned threads = (unsigned)(L < HASH_THREADS ? L : HASH_THREADS);
+    const int fuse = last ? 63 - __builtin_clzll(threads) : 0;
+    count_launch();
+    k_absorb_stripe<<<(unsigned)(L / threads), threads, 0, st>>>(stripe, L, ncols, cap, first, last, tree, fuse);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || !last) return e;
+    uint64_t m = L / threads;  // complete the tree above the block subtrees
+    while (m > 1) {
+        const uint64_t parents = m >> 1;
+        const unsigned th = (unsigned)(parents < UP_THREADS ? parents : UP_THREADS);
+        const int levels = 63 - __builtin_clzll(th) + 1;
+        count_launch();
+        k_merkle_up<<<(unsigned)(parents / th), th, 0, st>>>(tree, L, m, LAYOUT_HEAP, levels);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        m >>= levels;
+    }
+    return cudaSuccess;
 }
 
 }  // namespace tvmc

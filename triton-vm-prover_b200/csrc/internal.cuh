@@ -42,6 +42,11 @@ cudaError_t launch_merkle_from_leaves(uint64_t* tree, uint64_t n, int layout, cu
 // Copy n leaf digests into the tree's leaf slots and complete the tree.
 cudaError_t launch_merkle_tree(const uint64_t* leaves, uint64_t* tree, uint64_t n, int layout,
                                cudaStream_t st);
+// Frugal streaming: absorb ncols LDE columns (stride L) into per-row capacity
+// state cap[6][L]; `last` pads, finishes the digests as leaves of the heap tree
+// (2L digests) and builds the whole tree.
+cudaError_t launch_absorb_stripe(const uint64_t* stripe, uint64_t L, uint32_t ncols, uint64_t* cap, int first,
+                                 int last, uint64_t* tree, cudaStream_t st);
 cudaError_t launch_hash_pairs(const uint64_t* left, const uint64_t* right, uint64_t* out, uint64_t count,
                               cudaStream_t st);
 cudaError_t launch_tip5_permutations(uint64_t* states, uint64_t count, cudaStream_t st);

@@ -25,6 +25,7 @@ TRACE_ROW_MAJOR = 0x2
 DISCARD_LDE = 0x4
 SYNC = 0x8
 PROFILE = 0x10
+FRUGAL = 0x20
 
 _u64p = ctypes.POINTER(ctypes.c_uint64)
 _szp = ctypes.POINTER(ctypes.c_size_t)
@@ -91,6 +92,13 @@ SIGNATURES = {
     "tvmc_commitment_free": (ctypes.c_int, [_vp]),
     "tvmc_commitment_phase_ms": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_float)]),
     "tvmc_launch_count": (ctypes.c_ulonglong, []),
+    "tvmc_batch_create": (ctypes.c_int, [_vp, _sz, ctypes.POINTER(_vp)]),
+    "tvmc_batch_input": (ctypes.c_int, [_vp, _sz, ctypes.POINTER(_vp)]),
+    "tvmc_batch_run": (ctypes.c_int, [_vp, _vp]),
+    "tvmc_batch_commitment": (ctypes.c_int, [_vp, _sz, ctypes.POINTER(_vp)]),
+    "tvmc_batch_free": (ctypes.c_int, [_vp]),
+    "tvmc_set_tuning": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_longlong]),
+    "tvmc_get_tuning": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_longlong)]),
     "tvmc_int_peak_probe": (ctypes.c_double, [_vp]),
 }
 
@@ -180,6 +188,16 @@ def merkle_heap(leaves) -> np.ndarray:
     return nodes
 
 
+def set_tuning(key: str, value: int) -> None:
+    _check(lib().tvmc_set_tuning(key.encode(), int(value)))
+
+
+def get_tuning(key: str) -> int:
+    v = ctypes.c_longlong(0)
+    _check(lib().tvmc_get_tuning(key.encode(), ctypes.byref(v)))
+    return v.value
+
+
 def auth_structure_indices(num_leaves: int, leaves) -> np.ndarray:
     """Heap indices of MerkleTree::authentication_structure, descending (host only)."""
     ix = np.ascontiguousarray(leaves, dtype=np.uintp)
@@ -242,8 +260,8 @@ class Commitment:
 
     def __init__(self, trace, width: int | None = None, trace_len: int | None = None, expansion: int = 4,
                  offset: int = 7, row_major: bool = False, device_ptr: bool = False, discard_lde: bool = False,
-                 stream=None, sync: bool = False, profile: bool = False):
-        flags = PROFILE if profile else 0
+                 stream=None, sync: bool = False, profile: bool = False, frugal: bool = False):
+        flags = (PROFILE if profile else 0) | (FRUGAL if frugal else 0)
         if device_ptr:
             flags |= TRACE_DEVICE
             ptr = int(trace)
@@ -354,6 +372,75 @@ class Commitment:
             lib().tvmc_commitment_free(self.h)
             self.h = None
             self._keep = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.free()
+
+
+class TableShape(ctypes.Structure):
+    """tvmc_table_shape."""
+    _fields_ = [("trace_len", ctypes.c_size_t), ("width", ctypes.c_size_t), ("expansion", ctypes.c_uint32),
+                ("offset", ctypes.c_uint64)]
+
+
+class _BatchTable(Commitment):
+    """A batch-owned commitment handle: accessors only, freed with its batch."""
+
+    def __init__(self, h, width, trace_len, expansion):  # noqa: D401 - no commit here
+        self.h = h
+        self.width = width
+        self.trace_len = trace_len
+        self.lde_len = trace_len * expansion
+        self._keep = None
+
+    def free(self) -> None:
+        self.h = None
+
+
+class Batch:
+    """Many tables of uneven heights/widths committed by one CUDA-graph launch.
+
+    shapes: list of (trace_len, width[, expansion=4[, offset=7]])."""
+
+    def __init__(self, shapes):
+        norm = [tuple(s) + (4, 7)[len(s) - 2:] for s in shapes]
+        arr = (TableShape * len(norm))(*[TableShape(n, w, e, o) for n, w, e, o in norm])
+        h = _vp()
+        _check(lib().tvmc_batch_create(ctypes.cast(arr, _vp), len(norm), ctypes.byref(h)))
+        self.h = h
+        self.shapes = norm
+        self.tables = []
+        for i, (n, w, e, _o) in enumerate(norm):
+            c = _vp()
+            _check(lib().tvmc_batch_commitment(self.h, i, ctypes.byref(c)))
+            self.tables.append(_BatchTable(c, w, n, e))
+
+    def input_ptr(self, i: int) -> int:
+        p = _vp()
+        _check(lib().tvmc_batch_input(self.h, i, ctypes.byref(p)))
+        return p.value or 0
+
+    def run(self, stream=None) -> None:
+        _check(lib().tvmc_batch_run(self.h, _stream(stream)))
+
+    def roots(self) -> np.ndarray:
+        return np.stack([t.root() for t in self.tables])
+
+    def free(self) -> None:
+        if self.h is not None:
+            for t in self.tables:
+                t.free()
+            lib().tvmc_batch_free(self.h)
+            self.h = None
 
     def __del__(self):
         try:
