@@ -153,6 +153,9 @@ typedef struct tvmc_commitment tvmc_commitment;
  *                         (default: the widest stripe whose LDE fits in 2 GiB, at least 10)
  *   "lde_scratch_bytes"   LDE intermediate budget per call (default 2 GiB); columns are
  *                         processed in chunks that fit
+ *   "batch_streams"       worker streams a tvmc_batch spreads its tables over (default 8)
+ *   "lde_mid_ctas"        resident CTAs per SM for the fused LDE middle kernel: 2 (no register
+ *                         spills) or 3 (a few spills); default 2
  * Unknown keys return TVMC_ERR_INVALID. */
 int tvmc_set_tuning(const char* key, long long value);
 int tvmc_get_tuning(const char* key, long long* value);

@@ -413,24 +413,35 @@ struct tvmc_commitment {
     // TVMC_PROFILE: events at start / after upload / after LDE / after hash+tree
     cudaEvent_t prof[4] = {nullptr, nullptr, nullptr, nullptr};
     bool batch_owned = false;  // freed by tvmc_batch_free only
+    bool pooled = false;       // buffers from cudaMallocAsync on `stream`
 };
 
 namespace {
 void destroy_commitment(tvmc_commitment* c) {
-    if (c->done) {
-        cudaEventSynchronize(c->done);
-        cudaEventDestroy(c->done);
+    if (c->pooled) {
+        // ordered after the commitment's own work on its stream; the host does not wait
+        if (c->d_lde) cudaFreeAsync(c->d_lde, c->stream);
+        if (c->d_nodes) cudaFreeAsync(c->d_nodes, c->stream);
+        if (c->done) cudaEventDestroy(c->done);
     } else {
-        cudaStreamSynchronize(c->stream);
+        if (c->done) {
+            cudaEventSynchronize(c->done);
+            cudaEventDestroy(c->done);
+        } else {
+            cudaStreamSynchronize(c->stream);
+        }
+        if (c->d_lde) cudaFree(c->d_lde);
+        if (c->d_nodes) cudaFree(c->d_nodes);
     }
     for (auto ev : c->prof)
         if (ev) cudaEventDestroy(ev);
-    if (c->d_lde) cudaFree(c->d_lde);
-    if (c->d_nodes) cudaFree(c->d_nodes);
     delete c;
 }
 std::atomic<long long> g_tune_batch_streams{0};
+std::atomic<long long> g_tune_mid_ctas{0};
 }  // namespace
+
+int tvmc::tuning_lde_mid_ctas() { return g_tune_mid_ctas.load() == 3 ? 3 : 2; }
 
 struct tvmc_batch {
     int device = 0;
@@ -473,7 +484,10 @@ int tvmc_set_tuning(const char* key, long long value) {
     if (!strcmp(key, "frugal_stripe_cols")) g_tune_stripe_cols = value;
     else if (!strcmp(key, "lde_scratch_bytes")) g_tune_scratch_bytes = value;
     else if (!strcmp(key, "batch_streams")) g_tune_batch_streams = value;
-    else return fail(TVMC_ERR_INVALID, "unknown tuning key '%s'", key);
+    else if (!strcmp(key, "lde_mid_ctas")) {
+        if (value != 0 && value != 2 && value != 3) return fail(TVMC_ERR_INVALID, "lde_mid_ctas must be 0, 2 or 3");
+        g_tune_mid_ctas = value;
+    } else return fail(TVMC_ERR_INVALID, "unknown tuning key '%s'", key);
     return TVMC_OK;
 }
 
@@ -482,6 +496,7 @@ int tvmc_get_tuning(const char* key, long long* value) {
     if (!strcmp(key, "frugal_stripe_cols")) *value = g_tune_stripe_cols;
     else if (!strcmp(key, "lde_scratch_bytes")) *value = g_tune_scratch_bytes;
     else if (!strcmp(key, "batch_streams")) *value = g_tune_batch_streams;
+    else if (!strcmp(key, "lde_mid_ctas")) *value = g_tune_mid_ctas;
     else return fail(TVMC_ERR_INVALID, "unknown tuning key '%s'", key);
     return TVMC_OK;
 }
@@ -671,8 +686,11 @@ int tvmc_commit(const uint64_t* trace, size_t trace_len, size_t width, uint32_t 
     };
     const size_t NW = trace_len * width;
     const bool frugal = flags & TVMC_FRUGAL;
-    if (cudaMalloc((void**)&c->d_nodes, 2 * c->L * 40) != cudaSuccess ||
-        (width && !frugal && cudaMalloc((void**)&c->d_lde, c->L * width * 8) != cudaSuccess)) {
+    // stream-ordered pool memory: repeated commits reuse it without page mapping,
+    // and freeing a commitment never stalls the device
+    c->pooled = true;
+    if (cudaMallocAsync((void**)&c->d_nodes, 2 * c->L * 40, st) != cudaSuccess ||
+        (width && !frugal && cudaMallocAsync((void**)&c->d_lde, c->L * width * 8, st) != cudaSuccess)) {
         cudaGetLastError();
         return bail(fail(TVMC_ERR_NOMEM, "cannot allocate LDE (%zu x %zu) and tree", c->L, width));
     }

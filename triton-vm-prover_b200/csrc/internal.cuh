@@ -10,6 +10,9 @@ namespace tvmc {
 void count_launch();
 // Records `msg` as the calling thread's tvmc_last_error() text; returns code.
 int set_error(int code, const char* msg);
+// Tuning knob "lde_mid_ctas" (2 or 3 resident CTAs per SM for the fused LDE
+// middle kernel; default 2).
+int tuning_lde_mid_ctas();
 
 // Merkle node storage layouts.
 //   HEAP: 2n digests, node h at h (root 1, leaves [n, 2n), slot 0 unused) --

@@ -6,18 +6,21 @@
 // are canonical, so they equal the reference's radix-2 DIT bit for bit.
 //
 // Global structure.  Sizes up to 2^11 run in one pass per column (whole column
-// in shared memory).  Larger sizes use the four-step split n = n1*n2,
-// i = i1 + n1*i2, k = n2*k1 + k2:
+// in one CTA).  Larger sizes use the four-step split n = n1*n2, i = i1 + n1*i2,
+// k = n2*k1 + k2:
 //   pass A: for each i1, DFT_n2 over i2 (elements at stride n1), times w^(i1*k2)
 //   pass B: for each k2, DFT_n1 over i1 (contiguous rows) -> X[n2*k1 + k2]
 // A CTA moves T sequences at a time so that global accesses come in runs of T
 // consecutive words.
 //
-// In-CTA structure (sub_dft).  A sub-transform of size 2^LS <= 2^12 held in
-// shared memory is itself split four-step into rounds of radix <= 32; in each
-// round a thread loads one line of R elements into registers, runs a radix-2
-// DIF network there, applies the inter-round twiddle and writes the line back.
-// One __syncthreads per round instead of one per butterfly stage.
+// In-CTA structure (sub_dft).  A sub-transform of size 2^LS <= 2^12 is itself
+// split four-step into rounds of radix <= 32: in each round a thread holds one
+// line of R elements in registers and runs a radix-2 DIF network on it.  The
+// first round takes its inputs straight from a load function (global memory,
+// or shared memory times a scale) and the last round hands its outputs to a
+// store function (global memory times a twiddle), so shared memory carries only
+// the transposes between rounds: one write and one read per element per
+// round boundary, one barrier per boundary.
 //
 // LDE (LDE::extend_column, src/ntt/ntt.cpp:121-131; evaluate_on_coset :94-117):
 // the E*N-point forward transform of the zero-padded, offset-scaled
@@ -83,71 +86,129 @@ __device__ __forceinline__ void reg_dft(uint64_t (&v)[1 << B], const uint64_t* t
     }
 }
 
-// One round along the digit of stride S (elements lo + S*j + S*R*hi), for all
-// T x S x H lines.  MODE 0: no twiddle; 1: w^((d2*k) << b1) (first of three
-// rounds, d2 = lo >> b1); 2: w^(lo * (R3*k + hi)) (middle round).
-template <int LS, int B, int MODE>
-__device__ __forceinline__ void sub_round(uint64_t* s, int lT, const uint64_t* tw, int lS, int b1, int R3) {
-    constexpr int R = 1 << B;
+// DFT of size 2^LS on T = 2^lT sequences.  load(k, t) returns input element k
+// of sequence t (called once per element, by the first round); store(k, t, v)
+// receives output X[k] of sequence t (called once, by the last round).  With
+// TO_SMEM the last round instead writes X[k] back into s at element slot
+// out_pos<LS>(k) (the slots its line read), for a caller's rolled output loop
+// after a __syncthreads().  s is a shared buffer of spad_words(2^LS, lT) words
+// for the transposes between rounds and tw holds w^e, e < 2^LS.  Callers must
+// __syncthreads() before reusing s or before reading, in another thread,
+// anything a store wrote to shared memory.
+template <int LS, bool TO_SMEM = false, class LoadF, class StoreF>
+__device__ __forceinline__ void sub_dft(uint64_t* s, int lT, const uint64_t* tw, LoadF&& load, StoreF&& store) {
+    using PL = Plan<LS>;
     const int T = 1 << lT;
-    const int nlines = (1 << (LS - B)) << lT;
-    for (int id = threadIdx.x; id < nlines; id += blockDim.x) {
-        const int t = id & (T - 1);
-        const int rest = id >> lT;
-        const int lo = rest & ((1 << lS) - 1);
-        const int hi = rest >> lS;
-        const int base = lo + (hi << (lS + B));
-        uint64_t v[R];
+    if constexpr (PL::NR == 1) {
+        constexpr int R = 1 << LS;
+        for (int t = threadIdx.x; t < T; t += blockDim.x) {
+            uint64_t v[R];
 #pragma unroll
-        for (int j = 0; j < R; j++) v[j] = s[spos(base + (j << lS), lT) + t];
-        reg_dft<LS, B>(v, tw);
+            for (int j = 0; j < R; j++) v[j] = load(j, t);
+            reg_dft<LS, LS>(v, tw);
 #pragma unroll
-        for (int k = 0; k < R; k++) {
-            uint64_t x = v[brevc<B>(k)];
-            if (MODE == 1) {
-                const int e = ((lo >> b1) * k) << b1;
-                if (e) x = gl_mul_c(x, tw[e]);
-            } else if (MODE == 2) {
-                const int e = lo * (R3 * k + hi);
-                if (e) x = gl_mul_c(x, tw[e]);
+            for (int k = 0; k < R; k++) {
+                if constexpr (TO_SMEM) s[spos(k, lT) + t] = v[brevc<LS>(k)];
+                else store(k, t, v[brevc<LS>(k)]);
             }
-            s[spos(base + (k << lS), lT) + t] = x;
+        }
+    } else if constexpr (PL::NR == 2) {
+        constexpr int b1 = PL::b1, b2 = PL::b2, R1 = 1 << b1, R2 = 1 << b2;
+        // round 1: digit 2 (stride R1) for each (t, d1), twiddle w^(d1*k2)
+        for (int id = threadIdx.x; id < (R1 << lT); id += blockDim.x) {
+            const int t = id & (T - 1), d1 = id >> lT;
+            uint64_t v[R2];
+#pragma unroll
+            for (int j = 0; j < R2; j++) v[j] = load(d1 + (j << b1), t);
+            reg_dft<LS, b2>(v, tw);
+#pragma unroll
+            for (int k2 = 0; k2 < R2; k2++) {
+                uint64_t x = v[brevc<b2>(k2)];
+                if (k2) x = gl_mul_c(x, tw[d1 * k2]);
+                s[spos(d1 + (k2 << b1), lT) + t] = x;
+            }
+        }
+        __syncthreads();
+        // round 2: digit 1 (contiguous) for each (t, k2) -> X[R2*k1 + k2]
+        for (int id = threadIdx.x; id < (R2 << lT); id += blockDim.x) {
+            const int t = id & (T - 1), k2 = id >> lT;
+            uint64_t v[R1];
+#pragma unroll
+            for (int d1 = 0; d1 < R1; d1++) v[d1] = s[spos(d1 + (k2 << b1), lT) + t];
+            reg_dft<LS, b1>(v, tw);
+#pragma unroll
+            for (int k1 = 0; k1 < R1; k1++) {
+                if constexpr (TO_SMEM) s[spos(k1 + (k2 << b1), lT) + t] = v[brevc<b1>(k1)];
+                else store((k1 << b2) + k2, t, v[brevc<b1>(k1)]);
+            }
+        }
+    } else {
+        constexpr int b1 = PL::b1, b2 = PL::b2, b3 = PL::b3;
+        constexpr int R1 = 1 << b1, R2 = 1 << b2, R3 = 1 << b3;
+        // round A: digit 3 (stride R1*R2) for each (t, lo = d1 + R1*d2), twiddle w_{R2R3}^(d2*k3)
+        for (int id = threadIdx.x; id < ((R1 * R2) << lT); id += blockDim.x) {
+            const int t = id & (T - 1), lo = id >> lT;
+            uint64_t v[R3];
+#pragma unroll
+            for (int j = 0; j < R3; j++) v[j] = load(lo + (j << (b1 + b2)), t);
+            reg_dft<LS, b3>(v, tw);
+#pragma unroll
+            for (int k3 = 0; k3 < R3; k3++) {
+                uint64_t x = v[brevc<b3>(k3)];
+                const int e = ((lo >> b1) * k3) << b1;
+                if (e) x = gl_mul_c(x, tw[e]);
+                s[spos(lo + (k3 << (b1 + b2)), lT) + t] = x;
+            }
+        }
+        __syncthreads();
+        // round B: digit 2 (stride R1) for each (t, d1, k3), twiddle w^(d1*(R3*k2 + k3))
+        for (int id = threadIdx.x; id < ((R1 * R3) << lT); id += blockDim.x) {
+            const int t = id & (T - 1), rest = id >> lT;
+            const int d1 = rest & (R1 - 1), k3 = rest >> b1;
+            const int base = d1 + (k3 << (b1 + b2));
+            uint64_t v[R2];
+#pragma unroll
+            for (int j = 0; j < R2; j++) v[j] = s[spos(base + (j << b1), lT) + t];
+            reg_dft<LS, b2>(v, tw);
+#pragma unroll
+            for (int k2 = 0; k2 < R2; k2++) {
+                uint64_t x = v[brevc<b2>(k2)];
+                const int e = d1 * (R3 * k2 + k3);
+                if (e) x = gl_mul_c(x, tw[e]);
+                s[spos(base + (k2 << b1), lT) + t] = x;
+            }
+        }
+        __syncthreads();
+        // round C: digit 1 (contiguous) for each (t, k2, k3) -> X[R2R3*k1 + R3*k2 + k3]
+        for (int id = threadIdx.x; id < ((R2 * R3) << lT); id += blockDim.x) {
+            const int t = id & (T - 1), rest = id >> lT;
+            const int k2 = rest & (R2 - 1), k3 = rest >> b2;
+            uint64_t v[R1];
+#pragma unroll
+            for (int d1 = 0; d1 < R1; d1++) v[d1] = s[spos(d1 + (rest << b1), lT) + t];
+            reg_dft<LS, b1>(v, tw);
+#pragma unroll
+            for (int k1 = 0; k1 < R1; k1++) {
+                if constexpr (TO_SMEM) s[spos(k1 + (rest << b1), lT) + t] = v[brevc<b1>(k1)];
+                else store((k1 << (b2 + b3)) + R3 * k2 + k3, t, v[brevc<b1>(k1)]);
+            }
         }
     }
-    __syncthreads();
 }
 
-// DFT of size 2^LS of T sequences in shared memory, in place; X[k] ends at
-// element slot out_pos<LS>(k).  tw: 2^LS entries w^e in shared memory.
-template <int LS>
-__device__ __forceinline__ void sub_dft(uint64_t* s, int lT, const uint64_t* tw) {
-    using PL = Plan<LS>;
-    if constexpr (PL::NR == 1) {
-        sub_round<LS, PL::b1, 0>(s, lT, tw, 0, 0, 1);
-    } else if constexpr (PL::NR == 2) {
-        sub_round<LS, PL::b2, 2>(s, lT, tw, PL::b1, PL::b1, 1);
-        sub_round<LS, PL::b1, 0>(s, lT, tw, 0, 0, 1);
-    } else {
-        sub_round<LS, PL::b3, 1>(s, lT, tw, PL::b1 + PL::b2, PL::b1, 1);
-        sub_round<LS, PL::b2, 2>(s, lT, tw, PL::b1, PL::b1, 1 << PL::b3);
-        sub_round<LS, PL::b1, 0>(s, lT, tw, 0, 0, 1);
-    }
-}
-
+// Element slot of X[k] after sub_dft<LS, true>.
 template <int LS>
 __device__ __forceinline__ int out_pos(int k) {
     using PL = Plan<LS>;
     if constexpr (PL::NR == 1) {
         return k;
     } else if constexpr (PL::NR == 2) {
-        // X[R2*k1 + k2] sits at k1 + R1*k2
-        return (k >> PL::b2) + ((k & ((1 << PL::b2) - 1)) << PL::b1);
+        return (k >> PL::b2) + ((k & ((1 << PL::b2) - 1)) << PL::b1);  // X[R2*k1 + k2] at k1 + R1*k2
     } else {
-        // X[M*k1 + R3*k2 + k3] sits at k1 + R1*k2 + R1*R2*k3
-        const int k1 = k >> (PL::b2 + PL::b3);
+        const int k1 = k >> (PL::b2 + PL::b3);  // X[M*k1 + R3*k2 + k3] at k1 + R1*(k2 + R2*k3)
         const int k2 = (k >> PL::b3) & ((1 << PL::b2) - 1);
         const int k3 = k & ((1 << PL::b3) - 1);
-        return k1 + (k2 << PL::b1) + (k3 << (PL::b1 + PL::b2));
+        return k1 + ((k2 + (k3 << PL::b2)) << PL::b1);
     }
 }
 
@@ -164,29 +225,22 @@ __device__ __forceinline__ void load_tw(uint64_t* tw, const uint64_t* __restrict
 
 // ---------------------------------------------------------------- plain NTT
 
-// Whole columns in shared memory: T = 2^lT columns per CTA, size 2^LS <= 2^11.
+// Whole columns per CTA: T = 2^lT columns, size 2^LS <= 2^11, in place.
 template <int LS>
 __global__ void __launch_bounds__(NTT_THREADS) k_ntt_small(uint64_t* data, uint64_t ld, uint64_t cols, int lT,
                                                            const uint64_t* tw12, uint64_t scale) {
     extern __shared__ uint64_t sm[];
-    constexpr int n = 1 << LS;
-    const int T = 1 << lT;
     uint64_t* tw = sm;
-    uint64_t* s = sm + n;
+    uint64_t* s = sm + (1 << LS);
     load_tw<LS>(tw, tw12);
-    const uint64_t c0 = (uint64_t)blockIdx.x * T;
-    for (int idx = threadIdx.x; idx < n * T; idx += blockDim.x) {
-        const int t = idx >> LS, k = idx & (n - 1);  // coalesced along a column
-        const uint64_t col = c0 + t;
-        s[spos(k, lT) + t] = col < cols ? gl_canon(data[col * ld + k]) : 0;
-    }
     __syncthreads();
-    sub_dft<LS>(s, lT, tw);
-    for (int idx = threadIdx.x; idx < n * T; idx += blockDim.x) {
-        const int t = idx >> LS, k = idx & (n - 1);
-        const uint64_t col = c0 + t;
-        if (col < cols) data[col * ld + k] = gl_mul_c(s[spos(out_pos<LS>(k), lT) + t], scale);
-    }
+    const uint64_t c0 = (uint64_t)blockIdx.x << lT;
+    sub_dft<LS>(
+        s, lT, tw,
+        [&](int k, int t) { return c0 + t < cols ? gl_canon(data[(c0 + t) * ld + k]) : 0ull; },
+        [&](int k, int t, uint64_t v) {
+            if (c0 + t < cols) data[(c0 + t) * ld + k] = gl_mul_c(v, scale);
+        });
 }
 
 // Pass A: out[i1 + n1*k2] = w^(i1*k2) * DFT_n2(in[i1 + n1*i2])[k2]; in may equal out.
@@ -195,26 +249,21 @@ __global__ void __launch_bounds__(NTT_THREADS) k_pass_a(const uint64_t* in, uint
                                                         uint64_t old, int l1, int lT, const uint64_t* tw12,
                                                         const uint64_t* wlo, const uint64_t* whi) {
     extern __shared__ uint64_t sm[];
-    constexpr int n2 = 1 << L2;
-    const int T = 1 << lT;
     uint64_t* tw = sm;
-    uint64_t* s = sm + n2;
+    uint64_t* s = sm + (1 << L2);
     load_tw<L2>(tw, tw12);
-    const uint64_t col = blockIdx.y;
-    const uint32_t i10 = blockIdx.x << lT;
-    const uint64_t* src = in + col * ild;
-    for (int idx = threadIdx.x; idx < (n2 << lT); idx += blockDim.x) {
-        const int t = idx & (T - 1), i2 = idx >> lT;
-        s[spos(i2, lT) + t] = gl_canon(src[i10 + t + ((uint64_t)i2 << l1)]);
-    }
     __syncthreads();
-    sub_dft<L2>(s, lT, tw);
-    uint64_t* dst = out + col * old;
-    for (int idx = threadIdx.x; idx < (n2 << lT); idx += blockDim.x) {
+    const uint32_t i10 = blockIdx.x << lT;
+    const uint64_t* src = in + (uint64_t)blockIdx.y * ild + i10;
+    uint64_t* dst = out + (uint64_t)blockIdx.y * old + i10;
+    sub_dft<L2, true>(
+        s, lT, tw, [&](int k, int t) { return gl_canon(src[t + ((uint64_t)k << l1)]); }, [](int, int, uint64_t) {});
+    __syncthreads();
+    const int T = 1 << lT;
+    for (int idx = threadIdx.x; idx < (T << L2); idx += blockDim.x) {
         const int t = idx & (T - 1), k2 = idx >> lT;
-        uint64_t v = s[spos(out_pos<L2>(k2), lT) + t];
-        v = gl_mul_c(v, tw2(wlo, whi, (i10 + t) * (uint32_t)k2));
-        dst[i10 + t + ((uint64_t)k2 << l1)] = v;
+        const uint64_t v = s[spos(out_pos<L2>(k2), lT) + t];
+        dst[t + ((uint64_t)k2 << l1)] = gl_mul_c(v, tw2(wlo, whi, (i10 + t) * (uint32_t)k2));
     }
 }
 
@@ -224,31 +273,21 @@ __global__ void __launch_bounds__(NTT_THREADS) k_pass_b(const uint64_t* in, uint
                                                         uint64_t old, int l2, int lT, const uint64_t* tw12,
                                                         uint64_t scale) {
     extern __shared__ uint64_t sm[];
-    constexpr int n1 = 1 << L1;
-    const int T = 1 << lT;
     uint64_t* tw = sm;
-    uint64_t* s = sm + n1;
+    uint64_t* s = sm + (1 << L1);
     load_tw<L1>(tw, tw12);
-    const uint64_t col = blockIdx.y;
-    const uint32_t k20 = blockIdx.x << lT;
-    const uint64_t* src = in + col * ild + ((uint64_t)k20 << L1);
-    for (int idx = threadIdx.x; idx < (n1 << lT); idx += blockDim.x) {
-        const int t = idx >> L1, i1 = idx & (n1 - 1);  // coalesced along a row
-        s[spos(i1, lT) + t] = src[idx];
-    }
     __syncthreads();
-    sub_dft<L1>(s, lT, tw);
-    uint64_t* dst = out + col * old;
-    for (int idx = threadIdx.x; idx < (n1 << lT); idx += blockDim.x) {
-        const int t = idx & (T - 1), k1 = idx >> lT;
-        const uint64_t v = s[spos(out_pos<L1>(k1), lT) + t];
-        dst[((uint64_t)k1 << l2) + k20 + t] = gl_mul_c(v, scale);
-    }
+    const uint32_t k20 = blockIdx.x << lT;
+    const uint64_t* src = in + (uint64_t)blockIdx.y * ild + ((uint64_t)k20 << L1);
+    uint64_t* dst = out + (uint64_t)blockIdx.y * old + k20;
+    sub_dft<L1>(
+        s, lT, tw, [&](int k, int t) { return src[((uint64_t)t << L1) + k]; },
+        [&](int k, int t, uint64_t v) { dst[((uint64_t)k << l2) + t] = gl_mul_c(v, scale); });
 }
 
 // ---------------------------------------------------------------------- LDE
 
-// Small LDE: whole column in shared memory (N <= 2^11), T columns per CTA.
+// Small LDE: whole columns per CTA (N <= 2^11), T columns.
 template <int LS>
 __global__ void __launch_bounds__(NTT_THREADS) k_lde_small(const uint64_t* trace, uint64_t tld, uint64_t* out,
                                                            uint64_t old, uint64_t cols, int lT, int le,
@@ -257,35 +296,28 @@ __global__ void __launch_bounds__(NTT_THREADS) k_lde_small(const uint64_t* trace
                                                            int hi_len) {
     extern __shared__ uint64_t sm[];
     constexpr int n = 1 << LS;
-    const int T = 1 << lT, E = 1 << le;
+    const int E = 1 << le;
     uint64_t* twi = sm;
     uint64_t* twf = twi + n;
-    uint64_t* s = twf + n;                 // coefficients
-    uint64_t* w = s + spad_words(n, lT);   // work
+    uint64_t* cf = twf + n;                // coefficients (natural order)
+    uint64_t* s = cf + spad_words(n, lT);  // transposes
     load_tw<LS>(twi, tw12_i);
     load_tw<LS>(twf, tw12_f);
-    const uint64_t c0 = (uint64_t)blockIdx.x * T;
-    for (int idx = threadIdx.x; idx < n * T; idx += blockDim.x) {
-        const int t = idx >> LS, k = idx & (n - 1);
-        const uint64_t col = c0 + t;
-        s[spos(k, lT) + t] = col < cols ? gl_canon(trace[col * tld + k]) : 0;
-    }
     __syncthreads();
-    sub_dft<LS>(s, lT, twi);
+    const uint64_t c0 = (uint64_t)blockIdx.x << lT;
+    sub_dft<LS>(
+        s, lT, twi,
+        [&](int k, int t) { return c0 + t < cols ? gl_canon(trace[(c0 + t) * tld + k]) : 0ull; },
+        [&](int k, int t, uint64_t v) { cf[spos(k, lT) + t] = v; });
+    __syncthreads();
     for (int c = 0; c < E; c++) {
         const uint64_t* lo = sc_lo + 4096 * c;
         const uint64_t* hi = sc_hi + hi_len * c;
-        for (int idx = threadIdx.x; idx < n * T; idx += blockDim.x) {
-            const int t = idx & (T - 1), i = idx >> lT;
-            w[spos(i, lT) + t] = gl_mul_c(s[spos(out_pos<LS>(i), lT) + t], tw2(lo, hi, (uint32_t)i));
-        }
-        __syncthreads();
-        sub_dft<LS>(w, lT, twf);
-        for (int idx = threadIdx.x; idx < n * T; idx += blockDim.x) {
-            const int t = idx >> LS, q = idx & (n - 1);
-            const uint64_t col = c0 + t;
-            if (col < cols) out[col * old + (uint64_t)q * E + c] = w[spos(out_pos<LS>(q), lT) + t];
-        }
+        sub_dft<LS>(
+            s, lT, twf, [&](int k, int t) { return gl_mul_c(cf[spos(k, lT) + t], tw2(lo, hi, (uint32_t)k)); },
+            [&](int q, int t, uint64_t v) {
+                if (c0 + t < cols) out[(c0 + t) * old + (uint64_t)q * E + c] = v;
+            });
         __syncthreads();
     }
 }
@@ -296,25 +328,21 @@ __global__ void __launch_bounds__(NTT_THREADS) k_lde_inv_a(const uint64_t* trace
                                                            uint64_t yld, int l1, int lT, const uint64_t* tw12_i,
                                                            const uint64_t* wlo, const uint64_t* whi) {
     extern __shared__ uint64_t sm[];
-    constexpr int n2 = 1 << L2;
-    const int T = 1 << lT;
     uint64_t* tw = sm;
-    uint64_t* s = sm + n2;
+    uint64_t* s = sm + (1 << L2);
     load_tw<L2>(tw, tw12_i);
-    const uint64_t col = blockIdx.y;
-    const uint32_t i10 = blockIdx.x << lT;
-    const uint64_t* src = trace + col * tld;
-    for (int idx = threadIdx.x; idx < (n2 << lT); idx += blockDim.x) {
-        const int t = idx & (T - 1), i2 = idx >> lT;
-        s[spos(i2, lT) + t] = gl_canon(src[i10 + t + ((uint64_t)i2 << l1)]);
-    }
     __syncthreads();
-    sub_dft<L2>(s, lT, tw);
-    uint64_t* dst = Y + col * yld;
-    for (int idx = threadIdx.x; idx < (n2 << lT); idx += blockDim.x) {
+    const uint32_t i10 = blockIdx.x << lT;
+    const uint64_t* src = trace + (uint64_t)blockIdx.y * tld + i10;
+    uint64_t* dst = Y + (uint64_t)blockIdx.y * yld + i10;
+    sub_dft<L2, true>(
+        s, lT, tw, [&](int k, int t) { return gl_canon(src[t + ((uint64_t)k << l1)]); }, [](int, int, uint64_t) {});
+    __syncthreads();
+    const int T = 1 << lT;
+    for (int idx = threadIdx.x; idx < (T << L2); idx += blockDim.x) {
         const int t = idx & (T - 1), k2 = idx >> lT;
         const uint64_t v = s[spos(out_pos<L2>(k2), lT) + t];
-        dst[i10 + t + ((uint64_t)k2 << l1)] = gl_mul_c(v, tw2(wlo, whi, (i10 + t) * (uint32_t)k2));
+        dst[t + ((uint64_t)k2 << l1)] = gl_mul_c(v, tw2(wlo, whi, (i10 + t) * (uint32_t)k2));
     }
 }
 
@@ -329,81 +357,255 @@ __global__ void __launch_bounds__(NTT_THREADS) k_lde_mid(const uint64_t* Y, uint
                                                          const uint64_t* sc_hi, int hi_len) {
     extern __shared__ uint64_t sm[];
     constexpr int n1 = 1 << L1;
-    const int T = 1 << lT, E = 1 << le;
+    const int E = 1 << le;
     uint64_t* twi = sm;
     uint64_t* twf = twi + n1;
-    uint64_t* s = twf + n1;
-    uint64_t* w = s + spad_words(n1, lT);
+    uint64_t* cf = twf + n1;                 // coefficients, natural k1 order
+    uint64_t* s = cf + spad_words(n1, lT);   // transposes
     load_tw<L1>(twi, tw12_i);
     load_tw<L1>(twf, tw12_f);
+    __syncthreads();
     const uint64_t col = blockIdx.y;
     const uint32_t k20 = blockIdx.x << lT;
     const uint64_t* src = Y + col * yld + ((uint64_t)k20 << L1);
-    for (int idx = threadIdx.x; idx < (n1 << lT); idx += blockDim.x) {
-        const int t = idx >> L1, i1 = idx & (n1 - 1);
-        s[spos(i1, lT) + t] = src[idx];
-    }
+    sub_dft<L1>(
+        s, lT, twi, [&](int k, int t) { return src[((uint64_t)t << L1) + k]; },
+        [&](int k, int t, uint64_t v) { cf[spos(k, lT) + t] = v; });
     __syncthreads();
-    sub_dft<L1>(s, lT, twi);
     const uint64_t N = 1ull << (L1 + l2);
     for (int c = 0; c < E; c++) {
         const uint64_t* lo = sc_lo + 4096 * c;
         const uint64_t* hi = sc_hi + hi_len * c;
-        for (int idx = threadIdx.x; idx < (n1 << lT); idx += blockDim.x) {
-            const int t = idx & (T - 1), k1 = idx >> lT;
-            const uint32_t i = ((uint32_t)k1 << l2) + k20 + t;
-            w[spos(k1, lT) + t] = gl_mul_c(s[spos(out_pos<L1>(k1), lT) + t], tw2(lo, hi, i));
-        }
+        uint64_t* dst = Z + (col * E + c) * N + k20;
+        sub_dft<L1, true>(
+            s, lT, twf,
+            [&](int k, int t) {
+                return gl_mul_c(cf[spos(k, lT) + t], tw2(lo, hi, ((uint32_t)k << l2) + k20 + t));
+            },
+            [](int, int, uint64_t) {});
         __syncthreads();
-        sub_dft<L1>(w, lT, twf);
-        uint64_t* dst = Z + (col * E + c) * N;
-        for (int idx = threadIdx.x; idx < (n1 << lT); idx += blockDim.x) {
-            const int t = idx & (T - 1), q2 = idx >> lT;
-            uint64_t v = w[spos(out_pos<L1>(q2), lT) + t];
-            v = gl_mul_c(v, tw2(wlo, whi, (k20 + t) * (uint32_t)q2));
-            dst[k20 + t + ((uint64_t)q2 << l2)] = v;
+        const int T = 1 << lT;
+        for (int idx = threadIdx.x; idx < (T << L1); idx += blockDim.x) {
+            const int t = idx & (T - 1), q = idx >> lT;
+            const uint64_t v = s[spos(out_pos<L1>(q), lT) + t];
+            dst[t + ((uint64_t)q << l2)] = gl_mul_c(v, tw2(wlo, whi, (k20 + t) * (uint32_t)q));
         }
         __syncthreads();
     }
 }
 
+// K2 for two-round sub-transforms (n1 <= 2^10), 128 threads = T lines x R2.
+// The inverse DFT_n1 ends with thread (t, k) holding coefficients
+// c[R2*k1 + k], k1 < R1, in registers; splitting the forward DFT_n1 as
+// i = i1 + R2*i2 makes its first round take exactly that set (i1 = k), so the
+// coefficients stay in registers for all E cosets and only the forward's
+// second round goes through shared memory.
+template <int L1>
+__global__ void __launch_bounds__(128) k_lde_mid_reg(const uint64_t* Y, uint64_t yld, uint64_t* Z, int l2, int le,
+                                                     const uint64_t* tw12_i, const uint64_t* tw12_f,
+                                                     const uint64_t* wlo, const uint64_t* whi,
+                                                     const uint64_t* sc_lo, const uint64_t* sc_hi, int hi_len) {
+    using PL = Plan<L1>;
+    static_assert(PL::NR == 2, "two-round sizes only");
+    constexpr int b1 = PL::b1, b2 = PL::b2, R1 = 1 << b1, R2 = 1 << b2;
+    constexpr int lT = 7 - b2, T = 1 << lT;  // T * R2 = 128 threads
+    constexpr int n1 = 1 << L1;
+    extern __shared__ uint64_t sm[];
+    uint64_t* twi = sm;
+    uint64_t* twf = twi + n1;
+    uint64_t* s = twf + n1;
+    load_tw<L1>(twi, tw12_i);
+    load_tw<L1>(twf, tw12_f);
+    __syncthreads();
+    const int E = 1 << le;
+    const uint64_t col = blockIdx.y;
+    const uint32_t k20 = blockIdx.x << lT;
+    const uint64_t* src = Y + col * yld + ((uint64_t)k20 << L1);
+    // inverse, round 1: digit 2 (stride R1), lines (t, d1)
+    for (int id = threadIdx.x; id < (R1 << lT); id += blockDim.x) {
+        const int t = id & (T - 1), d1 = id >> lT;
+        uint64_t v[R2];
+#pragma unroll
+        for (int j = 0; j < R2; j++) v[j] = src[((uint64_t)t << L1) + d1 + (j << b1)];
+        reg_dft<L1, b2>(v, twi);
+#pragma unroll
+        for (int k2 = 0; k2 < R2; k2++) {
+            uint64_t x = v[brevc<b2>(k2)];
+            if (k2) x = gl_mul_c(x, twi[d1 * k2]);
+            s[spos(d1 + (k2 << b1), lT) + t] = x;
+        }
+    }
+    __syncthreads();
+    // inverse, round 2: this thread's line (t, kk) -> c[R2*k1 + kk]
+    const int t = threadIdx.x & (T - 1), kk = threadIdx.x >> lT;
+    uint64_t cf[R1];
+    {
+        uint64_t v[R1];
+#pragma unroll
+        for (int d1 = 0; d1 < R1; d1++) v[d1] = s[spos(d1 + (kk << b1), lT) + t];
+        reg_dft<L1, b1>(v, twi);
+#pragma unroll
+        for (int k1 = 0; k1 < R1; k1++) cf[k1] = v[brevc<b1>(k1)];
+    }
+    __syncthreads();
+    const uint64_t N = 1ull << (L1 + l2);
+    for (int c = 0; c < E; c++) {
+        const uint64_t* lo = sc_lo + 4096 * c;
+        const uint64_t* hi = sc_hi + hi_len * c;
+        // forward, round 1 on the register line: a[kk + R2*i2] * N^-1 s_c^i, DFT over i2
+        {
+            uint64_t v[R1];
+#pragma unroll
+            for (int k1 = 0; k1 < R1; k1++) {
+                const uint32_t ci = (uint32_t)kk + ((uint32_t)k1 << b2);
+                v[k1] = gl_mul_c(cf[k1], tw2(lo, hi, (ci << l2) + k20 + t));
+            }
+            reg_dft<L1, b1>(v, twf);
+#pragma unroll
+            for (int q = 0; q < R1; q++) {
+                uint64_t x = v[brevc<b1>(q)];
+                if (kk * q) x = gl_mul_c(x, twf[kk * q]);
+                s[spos(kk + (q << b2), lT) + t] = x;
+            }
+        }
+        __syncthreads();
+        // forward, round 2: lines (t, q2), DFT over i1 -> X[R1*q1 + q2] at slot q1 + R2*q2
+        for (int id = threadIdx.x; id < (R1 << lT); id += blockDim.x) {
+            const int tt = id & (T - 1), q2 = id >> lT;
+            uint64_t w[R2];
+#pragma unroll
+            for (int i1 = 0; i1 < R2; i1++) w[i1] = s[spos(i1 + (q2 << b2), lT) + tt];
+            reg_dft<L1, b2>(w, twf);
+#pragma unroll
+            for (int q1 = 0; q1 < R2; q1++) s[spos(q1 + (q2 << b2), lT) + tt] = w[brevc<b2>(q1)];
+        }
+        __syncthreads();
+        uint64_t* dst = Z + (col * E + c) * N + k20;
+        for (int idx = threadIdx.x; idx < (T << L1); idx += blockDim.x) {
+            const int tt = idx & (T - 1), q = idx >> lT;
+            const uint64_t x = s[spos((q >> b1) + ((q & (R1 - 1)) << b2), lT) + tt];
+            dst[tt + ((uint64_t)q << l2)] = gl_mul_c(x, tw2(wlo, whi, (k20 + tt) * (uint32_t)q));
+        }
+        __syncthreads();
+    }
+}
+
+// K2 for n1 = R*R (2^6, 2^8, 2^10): as k_lde_mid_reg, but the inverse and the
+// E forward transforms run through ONE rolled loop over (pass, round) around
+// a single register DFT body, so the kernel's code stays small enough for the
+// instruction cache.  Thread (t, ln) owns line ln of every round.
+template <int L1, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_lde_mid_sym(const uint64_t* Y, uint64_t yld, uint64_t* Z, int l2, int le,
+                                                     const uint64_t* tw12_i, const uint64_t* tw12_f,
+                                                     const uint64_t* wlo, const uint64_t* whi,
+                                                     const uint64_t* sc_lo, const uint64_t* sc_hi, int hi_len) {
+    using PL = Plan<L1>;
+    static_assert(PL::NR == 2 && PL::b1 == PL::b2, "square sizes only");
+    constexpr int B = PL::b1, R = 1 << B;
+    constexpr int lT = 7 - B, T = 1 << lT;  // T * R = 128 threads
+    constexpr int n1 = 1 << L1;
+    extern __shared__ uint64_t sm[];
+    uint64_t* twi = sm;
+    uint64_t* twf = twi + n1;
+    uint64_t* s = twf + n1;
+    load_tw<L1>(twi, tw12_i);
+    load_tw<L1>(twf, tw12_f);
+    __syncthreads();
+    const int E = 1 << le;
+    const uint64_t col = blockIdx.y;
+    const uint32_t k20 = blockIdx.x << lT;
+    const uint64_t* src = Y + col * yld + ((uint64_t)k20 << L1);
+    const uint64_t N = 1ull << (L1 + l2);
+    const int t = threadIdx.x & (T - 1), ln = threadIdx.x >> lT;
+    uint64_t cf[R];  // coefficients c[R*k1 + ln] of row k20 + t
+#pragma unroll 1
+    for (int pass = 0; pass <= E; pass++) {  // 0: inverse; c + 1: forward, coset c
+        const uint64_t* tw = pass ? twf : twi;
+        const uint64_t* lo = sc_lo + 4096 * (pass ? pass - 1 : 0);
+        const uint64_t* hi = sc_hi + hi_len * (pass ? pass - 1 : 0);
+#pragma unroll 1
+        for (int half = 0; half < 2; half++) {
+            uint64_t v[R];
+            if (half == 0) {
+                if (pass == 0) {  // inverse round 1: elements ln + R*j of row t
+#pragma unroll
+                    for (int j = 0; j < R; j++) v[j] = src[((uint64_t)t << L1) + ln + (j << B)];
+                } else {  // forward round 1: c[ln + R*k1] * N^-1 s_c^i
+#pragma unroll
+                    for (int k1 = 0; k1 < R; k1++) {
+                        const uint32_t ci = (uint32_t)ln + ((uint32_t)k1 << B);
+                        v[k1] = gl_mul_c(cf[k1], tw2(lo, hi, (ci << l2) + k20 + t));
+                    }
+                }
+            } else {  // round 2 of either: slots x + R*ln
+#pragma unroll
+                for (int x = 0; x < R; x++) v[x] = s[spos(x + (ln << B), lT) + t];
+            }
+            reg_dft<L1, B>(v, tw);
+            if (half == 0) {  // twiddle w^(ln*k), slot ln + R*k
+#pragma unroll
+                for (int k = 0; k < R; k++) {
+                    uint64_t x = v[brevc<B>(k)];
+                    if (ln * k) x = gl_mul_c(x, tw[ln * k]);
+                    s[spos(ln + (k << B), lT) + t] = x;
+                }
+            } else if (pass == 0) {
+#pragma unroll
+                for (int k1 = 0; k1 < R; k1++) cf[k1] = v[brevc<B>(k1)];
+            } else {  // X[R*q1 + ln] stays in slot q1 + R*ln
+#pragma unroll
+                for (int q1 = 0; q1 < R; q1++) s[spos(q1 + (ln << B), lT) + t] = v[brevc<B>(q1)];
+            }
+            __syncthreads();
+        }
+        if (pass) {
+            uint64_t* dst = Z + (col * E + pass - 1) * N + k20;
+            for (int idx = threadIdx.x; idx < (T << L1); idx += blockDim.x) {
+                const int tt = idx & (T - 1), q = idx >> lT;
+                const uint64_t x = s[spos((q >> B) + ((q & (R - 1)) << B), lT) + tt];
+                dst[tt + ((uint64_t)q << l2)] = gl_mul_c(x, tw2(wlo, whi, (k20 + tt) * (uint32_t)q));
+            }
+            __syncthreads();
+        }
+    }
+}
+
 // K3: for q2 in [q20, q20+T3), all E cosets: DFT_n2 over rows Z_c[i1' + n2*q2];
 // E_c[n1*q1 + q2] -> LDE[E*(n1*q1 + q2) + c], written as runs of E*T3 words.
+// Sequence u = E*t + c of the CTA is row q20 + t of coset c.
 template <int L2>
 __global__ void __launch_bounds__(NTT_THREADS) k_lde_fwd_b(const uint64_t* Z, uint64_t* out, uint64_t old,
                                                            int l1, int lT3, int le, const uint64_t* tw12_f) {
     extern __shared__ uint64_t sm[];
-    constexpr int n2 = 1 << L2;
-    const int T3 = 1 << lT3, E = 1 << le;
-    const int lS = lT3 + le;  // sequences per CTA = E*T3, seq u = E*t + c
+    const int E = 1 << le;
+    const int lS = lT3 + le;
     uint64_t* tw = sm;
-    uint64_t* s = sm + n2;
+    uint64_t* s = sm + (1 << L2);
     load_tw<L2>(tw, tw12_f);
+    __syncthreads();
     const uint64_t col = blockIdx.y;
     const uint32_t q20 = blockIdx.x << lT3;
     const uint64_t N = 1ull << (l1 + L2);
-    for (int idx = threadIdx.x; idx < (n2 << lS); idx += blockDim.x) {
-        const int seq = idx >> L2, i1 = idx & (n2 - 1);
-        const int c = seq >> lT3, t = seq & (T3 - 1);
-        const uint64_t v = Z[(col * E + c) * N + ((uint64_t)(q20 + t) << L2) + i1];
-        s[spos(i1, lS) + (t << le) + c] = v;
-    }
-    __syncthreads();
-    sub_dft<L2>(s, lS, tw);
-    uint64_t* dst = out + col * old;
-    const int S = 1 << lS;
-    for (int idx = threadIdx.x; idx < (n2 << lS); idx += blockDim.x) {
-        const int u = idx & (S - 1), q1 = idx >> lS;
-        dst[(((uint64_t)q1 << l1) + q20) * E + u] = s[spos(out_pos<L2>(q1), lS) + u];
-    }
+    const uint64_t* src = Z + col * E * N + ((uint64_t)q20 << L2);
+    uint64_t* dst = out + col * old + (uint64_t)q20 * E;
+    sub_dft<L2>(
+        s, lS, tw,
+        [&](int k, int u) {
+            const int c = u & (E - 1), t = u >> le;
+            return src[(uint64_t)c * N + ((uint64_t)t << L2) + k];
+        },
+        [&](int q, int u, uint64_t v) { dst[(((uint64_t)q << l1) * E) + u] = v; });
 }
 
 // ------------------------------------------------------------------ helpers
 
 static inline int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
-// T = 2^lT sequences so that T * 2^ls ~ 2^budget, within [1, 8].
-static int choose_lT(int ls, int budget_words_log) { return clampi(budget_words_log - ls, 0, 3); }
+// T = 2^lT sequences so that T * 2^ls ~ 2^budget.  Sizes up to 2^5 run as one
+// register round per sequence, so they take up to 256 sequences per CTA.
+static int choose_lT(int ls, int budget_words_log) {
+    return clampi(budget_words_log - ls, 0, ls <= 5 ? 8 : 3);
+}
 
 static cudaError_t set_smem(const void* fn, size_t bytes) {
     if (bytes > 48 * 1024)
@@ -539,11 +741,31 @@ cudaError_t launch_lde(const LdePlan& pl, const uint64_t* trace, uint64_t tld, u
         });
         if (e != cudaSuccess) return e;
         e = dispatch_ls(l1, [&]<int L1>() -> cudaError_t {
-            cudaError_t e2 = set_smem((const void*)k_lde_mid<L1>, smem2);
-            if (e2 != cudaSuccess) return e2;
-            count_launch();
-            k_lde_mid<L1><<<dim3((1u << l2) >> lT2, nc), NTT_THREADS, smem2, st>>>(
-                Y, N, Z, l2, lT2, le, pl.tw12_i, pl.tw12_f, pl.wn_f_lo, pl.wn_f_hi, pl.sc_lo, pl.sc_hi, hi_len);
+            if constexpr (Plan<L1>::NR == 2 && Plan<L1>::b1 == Plan<L1>::b2) {
+                constexpr int lTr = 7 - Plan<L1>::b2;
+                const size_t smr = words_bytes(2 * (size_t)(1u << L1) + spad_words(1 << L1, lTr));
+                // register budget: 2 resident CTAs (no spills) or 3 (a few spills); tuning knob
+                auto kern = tuning_lde_mid_ctas() == 3 ? k_lde_mid_sym<L1, 3> : k_lde_mid_sym<L1, 2>;
+                cudaError_t e2 = set_smem((const void*)kern, smr);
+                if (e2 != cudaSuccess) return e2;
+                count_launch();
+                kern<<<dim3((1u << l2) >> lTr, nc), 128, smr, st>>>(
+                    Y, N, Z, l2, le, pl.tw12_i, pl.tw12_f, pl.wn_f_lo, pl.wn_f_hi, pl.sc_lo, pl.sc_hi, hi_len);
+            } else if constexpr (Plan<L1>::NR == 2) {
+                constexpr int lTr = 7 - Plan<L1>::b2;
+                const size_t smr = words_bytes(2 * (size_t)(1u << L1) + spad_words(1 << L1, lTr));
+                cudaError_t e2 = set_smem((const void*)k_lde_mid_reg<L1>, smr);
+                if (e2 != cudaSuccess) return e2;
+                count_launch();
+                k_lde_mid_reg<L1><<<dim3((1u << l2) >> lTr, nc), 128, smr, st>>>(
+                    Y, N, Z, l2, le, pl.tw12_i, pl.tw12_f, pl.wn_f_lo, pl.wn_f_hi, pl.sc_lo, pl.sc_hi, hi_len);
+            } else {
+                cudaError_t e2 = set_smem((const void*)k_lde_mid<L1>, smem2);
+                if (e2 != cudaSuccess) return e2;
+                count_launch();
+                k_lde_mid<L1><<<dim3((1u << l2) >> lT2, nc), NTT_THREADS, smem2, st>>>(
+                    Y, N, Z, l2, lT2, le, pl.tw12_i, pl.tw12_f, pl.wn_f_lo, pl.wn_f_hi, pl.sc_lo, pl.sc_hi, hi_len);
+            }
             return cudaGetLastError();
         });
         if (e != cudaSuccess) return e;
