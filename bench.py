@@ -288,6 +288,12 @@ def run_ours(args):
     if os.path.exists(peaks_path):
         hbm_peak, hbm_src = float(json.load(open(peaks_path))["hbm_gbs"]), "measured"
     int_peak = int_peak_tops(torch, dev)
+    # DRAM bytes per k_hash_rows launch: one ncu capture of the 2^18-row x 379-column
+    # main-table launch (796.1 MB read + 20.5 MB written), scaled by rows
+    traffic, traffic_src = None, None
+    if W_MAIN == 379:
+        traffic = (796.1e6 + 20.5e6) * L / (1 << 18)
+        traffic_src = "ncu dram__bytes_read+write of a 2^18x379 launch, scaled by LDE rows (main table)"
 
     # e2e: pinned host traces through the public C ABI, roots read back
     e2e = None
@@ -342,13 +348,13 @@ def run_ours(args):
                                    "Tip5 row hash, Merkle (two trees)",
                        "trace_len": n, "lde_len": L, "widths": [W_MAIN, W_AUX], "expansion": EXPANSION,
                        "cells_per_step": cells_step, "l2": "inputs (5.4 GB) larger than L2",
-                       "tuning": tuned.get("knobs", {}),
+                       "tuning": tuned.get("knobs", {}), "tuning_s": tuned.get("seconds", {}),
                        "parallelism": "replicas" if ws > 1 else "1 gpu"},
             "roofline": {"bound": "int32", "kernel": "k_hash_rows + k_merkle_up (Tip5)",
                          "achieved": achieved_int, "peak": int_peak, "unit": "Top/s",
                          "frac": achieved_int / int_peak if int_peak == int_peak else None,
                          "peak_source": "measured int32 issue probe (tvmc_int_peak_probe)",
-                         "traffic": None, "cost_model": f"{OPS_PER_PERM} int32 ops per Tip5 permutation",
+                         "traffic": traffic, "traffic_source": traffic_src, "cost_model": f"{OPS_PER_PERM} int32 ops per Tip5 permutation",
                          "ms_per_step": sum(hash_ms) / args.steps},
             "roofline_lde": {"bound": "hbm", "achieved": achieved_hbm, "peak": hbm_peak, "unit": "GB/s",
                              "frac": achieved_hbm / hbm_peak, "peak_source": hbm_src,

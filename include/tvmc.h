@@ -156,6 +156,8 @@ typedef struct tvmc_commitment tvmc_commitment;
  *   "batch_streams"       worker streams a tvmc_batch spreads its tables over (default 8)
  *   "lde_mid_ctas"        resident CTAs per SM for the fused LDE middle kernel: 2 (no register
  *                         spills) or 3 (a few spills); default 2
+ *   "hash_unfused_tree"   1: build every Merkle level in the tree kernel instead of the lowest
+ *                         eight inside the row-hash CTAs; default 0
  * Unknown keys return TVMC_ERR_INVALID. */
 int tvmc_set_tuning(const char* key, long long value);
 int tvmc_get_tuning(const char* key, long long* value);

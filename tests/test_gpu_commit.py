@@ -111,3 +111,21 @@ def test_commit_full_size_properties(tv, oracle):
         for i, lf, p in zip(idx, leaves, paths):
             assert oracle.verify(root, int(i), lf, p)
         assert (root < P).all()
+
+
+@pytest.mark.parametrize("knob,value", [("hash_unfused_tree", 1), ("lde_mid_ctas", 3)])
+@pytest.mark.parametrize("logn", [4, 12, 14])
+def test_tuning_knobs_do_not_change_results(tv, oracle, knob, value, logn):
+    """Scheduling knobs change no bit: plain and frugal commits vs the default."""
+    t = rand_u64(0xC0FFEE + logn, (23, 1 << logn))
+    with tv.Commitment(t) as ref:
+        exp = ref.nodes()
+    try:
+        tv.set_tuning(knob, value)
+        with tv.Commitment(t) as a, tv.Commitment(t, frugal=True) as b:
+            assert (a.nodes()[1:] == exp[1:]).all()
+            assert (b.nodes()[1:] == exp[1:]).all()
+    finally:
+        tv.set_tuning(knob, 0)
+    if logn == 4:
+        assert (exp[1:] == oracle.merkle(oracle.hash_rows_cm(oracle.lde(t)))[1:]).all()

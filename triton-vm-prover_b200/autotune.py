@@ -5,6 +5,7 @@ caller's own table shapes, keeps the fastest, and persists the choice in a JSON
 cache keyed by device name and shape, so later processes start tuned:
 
     lde_mid_ctas        resident CTAs/SM of the fused LDE middle kernel (2, 3)
+    hash_unfused_tree   1 = build all Merkle levels in the tree kernel (0, 1)
     batch_streams       worker streams of a tvmc_batch (1 .. 16)
     frugal_stripe_cols  columns per frugal stripe (multiples of 10)
 
@@ -73,19 +74,22 @@ def tune_commit(trace_ptr: int, trace_len: int, width: int, expansion: int = 4, 
     if key in db and not force:
         apply(db[key]["knobs"])
         return db[key]
+
+    def run():
+        c = tvmc.Commitment(trace_ptr, width=width, trace_len=trace_len, device_ptr=True,
+                            expansion=expansion, offset=offset, stream=stream)
+        c.sync()
+        c.free()
+
     results = {}
     for ctas in (2, 3):
-        tvmc.set_tuning("lde_mid_ctas", ctas)
-
-        def run():
-            c = tvmc.Commitment(trace_ptr, width=width, trace_len=trace_len, device_ptr=True,
-                                expansion=expansion, offset=offset, stream=stream)
-            c.sync()
-            c.free()
-
-        results[ctas] = _time(run)
+        for unfused in (0, 1):
+            tvmc.set_tuning("lde_mid_ctas", ctas)
+            tvmc.set_tuning("hash_unfused_tree", unfused)
+            results[(ctas, unfused)] = _time(run)
     best = min(results, key=results.get)
-    entry = {"knobs": {"lde_mid_ctas": best}, "seconds": {str(k): v for k, v in results.items()}}
+    entry = {"knobs": {"lde_mid_ctas": best[0], "hash_unfused_tree": best[1]},
+             "seconds": {f"{k[0]},{k[1]}": v for k, v in results.items()}}
     apply(entry["knobs"])
     db[key] = entry
     save(db, path)

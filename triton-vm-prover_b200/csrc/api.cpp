@@ -439,9 +439,11 @@ void destroy_commitment(tvmc_commitment* c) {
 }
 std::atomic<long long> g_tune_batch_streams{0};
 std::atomic<long long> g_tune_mid_ctas{0};
+std::atomic<long long> g_tune_unfused_tree{0};
 }  // namespace
 
 int tvmc::tuning_lde_mid_ctas() { return g_tune_mid_ctas.load() == 3 ? 3 : 2; }
+int tvmc::tuning_hash_fuse_levels() { return g_tune_unfused_tree.load() ? 0 : 8; }
 
 struct tvmc_batch {
     int device = 0;
@@ -487,7 +489,8 @@ int tvmc_set_tuning(const char* key, long long value) {
     else if (!strcmp(key, "lde_mid_ctas")) {
         if (value != 0 && value != 2 && value != 3) return fail(TVMC_ERR_INVALID, "lde_mid_ctas must be 0, 2 or 3");
         g_tune_mid_ctas = value;
-    } else return fail(TVMC_ERR_INVALID, "unknown tuning key '%s'", key);
+    } else if (!strcmp(key, "hash_unfused_tree")) g_tune_unfused_tree = value ? 1 : 0;
+    else return fail(TVMC_ERR_INVALID, "unknown tuning key '%s'", key);
     return TVMC_OK;
 }
 
@@ -497,6 +500,7 @@ int tvmc_get_tuning(const char* key, long long* value) {
     else if (!strcmp(key, "lde_scratch_bytes")) *value = g_tune_scratch_bytes;
     else if (!strcmp(key, "batch_streams")) *value = g_tune_batch_streams;
     else if (!strcmp(key, "lde_mid_ctas")) *value = g_tune_mid_ctas;
+    else if (!strcmp(key, "hash_unfused_tree")) *value = g_tune_unfused_tree;
     else return fail(TVMC_ERR_INVALID, "unknown tuning key '%s'", key);
     return TVMC_OK;
 }

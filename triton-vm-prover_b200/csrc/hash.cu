@@ -284,14 +284,14 @@ cudaError_t launch_hash_rows(const uint64_t* table, uint64_t rstride, uint64_t c
         return cudaGetLastError();
     }
     unsigned threads = (unsigned)(rows < HASH_THREADS ? rows : HASH_THREADS);
-    int fuse = ilog2u(threads);
+    const int fuse = ilog2u(threads) < tuning_hash_fuse_levels() ? ilog2u(threads) : tuning_hash_fuse_levels();
     count_launch();
     k_hash_rows<<<grid_for(rows, threads), threads, 0, st>>>(table, rstride, cstride, rows, width, nullptr, tree,
                                                              layout, fuse);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    // the block subtrees are complete; continue from the level of rows/threads nodes
-    uint64_t m = rows / threads;
+    // the block subtrees are complete up to `fuse` levels; continue from there
+    uint64_t m = rows >> fuse;
     while (m > 1) {
         uint64_t parents = m >> 1;
         unsigned th = (unsigned)(parents < UP_THREADS ? parents : UP_THREADS);
@@ -357,12 +357,13 @@ cudaError_t launch_gather_rows(const uint64_t* table, uint64_t ld, uint32_t widt
 cudaError_t launch_absorb_stripe(const uint64_t* stripe, uint64_t L, uint32_t ncols, uint64_t* cap, int first,
                                  int last, uint64_t* tree, cudaStream_t st) {
     const unsigned threads = (unsigned)(L < HASH_THREADS ? L : HASH_THREADS);
-    const int fuse = last ? 63 - __builtin_clzll(threads) : 0;
+    const int lt = 63 - __builtin_clzll(threads);
+    const int fuse = last ? (lt < tuning_hash_fuse_levels() ? lt : tuning_hash_fuse_levels()) : 0;
     count_launch();
     k_absorb_stripe<<<(unsigned)(L / threads), threads, 0, st>>>(stripe, L, ncols, cap, first, last, tree, fuse);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess || !last) return e;
-    uint64_t m = L / threads;  // complete the tree above the block subtrees
+    uint64_t m = L >> fuse;  // complete the tree above the block subtrees
     while (m > 1) {
         const uint64_t parents = m >> 1;
         const unsigned th = (unsigned)(parents < UP_THREADS ? parents : UP_THREADS);

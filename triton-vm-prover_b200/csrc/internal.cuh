@@ -13,6 +13,9 @@ int set_error(int code, const char* msg);
 // Tuning knob "lde_mid_ctas" (2 or 3 resident CTAs per SM for the fused LDE
 // middle kernel; default 2).
 int tuning_lde_mid_ctas();
+// Merkle levels built inside the row-hash CTA (8 by default; 0 with the tuning
+// knob "hash_unfused_tree" = 1); the rest are built by k_merkle_up.
+int tuning_hash_fuse_levels();
 
 // Merkle node storage layouts.
 //   HEAP: 2n digests, node h at h (root 1, leaves [n, 2n), slot 0 unused) --
