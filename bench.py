@@ -355,11 +355,13 @@ def run_ours(args):
                          "frac": achieved_int / int_peak if int_peak == int_peak else None,
                          "peak_source": "measured int32 issue probe (tvmc_int_peak_probe)",
                          "traffic": traffic, "traffic_source": traffic_src, "cost_model": f"{OPS_PER_PERM} int32 ops per Tip5 permutation",
-                         "ms_per_step": sum(hash_ms) / args.steps},
+                         "ms_per_step": sum(hash_ms) / args.steps,
+                         "ms_per_table_min_max": [min(hash_ms), max(hash_ms)]},
             "roofline_lde": {"bound": "hbm", "achieved": achieved_hbm, "peak": hbm_peak, "unit": "GB/s",
                              "frac": achieved_hbm / hbm_peak, "peak_source": hbm_src,
                              "bytes": "8*N*W read + 8*4N*W written per table",
-                             "ms_per_step": sum(lde_ms) / args.steps},
+                             "ms_per_step": sum(lde_ms) / args.steps,
+                             "ms_per_table_min_max": [min(lde_ms), max(lde_ms)]},
             "e2e": e2e,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),

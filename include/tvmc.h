@@ -69,6 +69,15 @@ int tvmc_ntt_forward_batched_gpu(uint64_t* d_data, size_t n, size_t num_cols, vo
 int tvmc_ntt_inverse_batched_gpu(uint64_t* d_data, size_t n, size_t num_cols, void* stream);
 /* Host-buffer form of the two above (NTT::forward / NTT::inverse on each column). */
 int tvmc_ntt_host(uint64_t* data, size_t n, size_t num_cols, int inverse);
+/* NTT::evaluate_on_coset (src/ntt/ntt.cpp:94-117) of num_cols coefficient
+ * columns (d_coeffs[col*num_coeffs + i]): the first min(num_coeffs, domain_len)
+ * coefficients, zero-extended to domain_len and scaled by offset^i, forward
+ * NTT; d_out[col*domain_len + j] = f(offset * w^j). */
+int tvmc_evaluate_on_coset_gpu(const uint64_t* d_coeffs, size_t num_coeffs, size_t num_cols, uint64_t* d_out,
+                               size_t domain_len, uint64_t offset, void* stream);
+/* Host-buffer form. */
+int tvmc_evaluate_on_coset_host(const uint64_t* coeffs, size_t num_coeffs, size_t num_cols, uint64_t* out,
+                                size_t domain_len, uint64_t offset);
 
 /* ---- LDE (include/gpu/kernels/lde_kernel.cuh lde_batch_gpu; src/ntt/ntt.cpp:121-131) ---- */
 
@@ -82,6 +91,22 @@ int tvmc_lde_batch_gpu(const uint64_t* d_traces, size_t num_columns, size_t trac
 /* Host-buffer form (LDE::extend_table on column-major data). */
 int tvmc_lde_host(const uint64_t* traces, size_t num_columns, size_t trace_len, uint64_t* extended,
                   size_t extended_len, uint64_t extended_offset);
+
+/* Randomized LDE (RandomizedLDE::extend_column_with_randomizer,
+ * src/lde/lde_randomized.cpp:71-154; the GPU counterpart is the randomized LDE
+ * of src/gpu/gpu_stark.cu:2132-2617): interpolant of each column on
+ * trace_offset * <w_trace_len> (the trace offset is honoured here), plus
+ * (x^trace_len - trace_offset^trace_len) * r(x) with r's num_randomizers
+ * coefficients at d_randomizers[col*num_randomizers + k], evaluated on
+ * extended_offset * <w_extended_len>.  flags: 0 or TVMC_RAND_TRUNCATE. */
+int tvmc_lde_randomized_gpu(const uint64_t* d_traces, size_t num_columns, size_t trace_len,
+                            const uint64_t* d_randomizers, size_t num_randomizers, uint64_t* d_extended,
+                            size_t extended_len, uint64_t trace_offset, uint64_t extended_offset, uint32_t flags,
+                            void* stream);
+/* Host-buffer form. */
+int tvmc_lde_randomized_host(const uint64_t* traces, size_t num_columns, size_t trace_len,
+                             const uint64_t* randomizers, size_t num_randomizers, uint64_t* extended,
+                             size_t extended_len, uint64_t trace_offset, uint64_t extended_offset, uint32_t flags);
 
 /* Words (64 MiB) of the static device array used by tvmc_lde_batch_noalloc_gpu. */
 #define TVMC_NOALLOC_SCRATCH_WORDS ((size_t)1 << 23)
@@ -122,6 +147,16 @@ int tvmc_hash_pairs_host(const uint64_t* left, const uint64_t* right, uint64_t* 
  * (Backend::tip5_permutation_batch, include/backend/backend.hpp:99-104). */
 int tvmc_tip5_permutation_batch_gpu(uint64_t* d_states, size_t num_states, void* stream);
 int tvmc_tip5_permutation_batch_host(uint64_t* states, size_t num_states);
+/* Tip5::round for rounds [first_round, first_round + num_rounds) of each state
+ * (src/hash/tip5.cpp:114-118); with a non-null trace, the state after each
+ * round goes to trace[(i*num_rounds + k)*16 + .] (Tip5::trace, :97-112). */
+int tvmc_tip5_rounds_host(uint64_t* states, size_t num_states, uint32_t first_round, uint32_t num_rounds,
+                          uint64_t* trace);
+/* The Tip5 parameters this library computes with: the 256-byte S-box lookup
+ * table, the MDS matrix's first column and the 80 round constants
+ * (Tip5::LOOKUP_TABLE, MDS_MATRIX_FIRST_COLUMN, ROUND_CONSTANTS,
+ * src/hash/tip5.cpp:7-79).  Host only; any pointer may be null. */
+int tvmc_tip5_parameters(uint8_t* lookup_table, uint64_t* mds_first_column, uint64_t* round_constants);
 
 /* ---- Merkle (include/gpu/kernels/merkle_kernel.cuh:26-50, src/merkle/merkle_tree.cpp) ---- */
 
@@ -133,6 +168,15 @@ int tvmc_merkle_root_gpu(const uint64_t* d_leaves, uint64_t* d_root, size_t num_
 /* Heap layout, as the reference's CPU MerkleTree: nodes holds 2n digests,
  * node 1 is the root, leaves at [n, 2n), node 0 is written as zeros. */
 int tvmc_merkle_tree_heap_host(const uint64_t* leaves, size_t num_leaves, uint64_t* nodes);
+/* Root implied by each (leaf index, leaf digest, authentication path) triple,
+ * as MerkleTree::verify walks it (src/merkle/merkle_tree.cpp:343-364): sibling
+ * k of triple q at paths[(q*path_len + k)*5 + .]; roots[q*5 + .].  A path
+ * verifies iff its root equals the tree's. */
+int tvmc_merkle_root_from_paths_gpu(const size_t* d_leaf_idx, const uint64_t* d_leaves, const uint64_t* d_paths,
+                                    size_t count, size_t path_len, uint64_t* d_roots, void* stream);
+/* Host-buffer form. */
+int tvmc_merkle_root_from_paths_host(const size_t* leaf_idx, const uint64_t* leaves, const uint64_t* paths,
+                                     size_t count, size_t path_len, uint64_t* roots);
 
 /* ---- table commitment (the whole path; src/gpu/gpu_stark.cu:2132-2617 step 2/3,
  *      src/stark.cpp:1163-1196, LDETable::compute_lde_and_merkle src/lde/lde_table.cpp:86-101) ---- */
@@ -147,6 +191,11 @@ typedef struct tvmc_commitment tvmc_commitment;
 #define TVMC_FRUGAL 0x20u         /* streaming mode: LDE in 10-column-aligned stripes absorbed into
                                      resident sponge states; the full LDE is never stored (implies
                                      TVMC_DISCARD_LDE); for very tall tables (2^22 rows and up) */
+#define TVMC_RAND_TRUNCATE 0x40u  /* randomized LDE: drop coefficients of degree >= the LDE length
+                                     before evaluating, as the reference's XFieldElement variants do
+                                     (RandomizedLDE::extend_xfield_column_with_randomizer,
+                                     src/lde/lde_randomized.cpp:246-251); otherwise a longer
+                                     polynomial is evaluated exactly (chunked, :120-153) */
 
 /* Tuning knobs (process-wide; 0 restores the default):
  *   "frugal_stripe_cols"  columns per TVMC_FRUGAL stripe, rounded down to a multiple of 10
@@ -169,6 +218,18 @@ int tvmc_get_tuning(const char* key, long long* value);
  * tvmc_commitment_free.  Work is enqueued on `stream`. */
 int tvmc_commit(const uint64_t* trace, size_t trace_len, size_t width, uint32_t expansion, uint64_t offset,
                 uint32_t flags, void* stream, tvmc_commitment** out);
+/* The same commitment over the randomized (zero-knowledge) LDE of
+ * LDETable::extend_table_with_randomizers / RandomizedLDE::extend_column_with_randomizer
+ * (src/lde/lde_table.cpp:8-57, src/lde/lde_randomized.cpp:71-154): per column
+ * the interpolant on trace_offset * <w_trace_len> plus (x^trace_len - trace_offset^trace_len)
+ * times the randomizer polynomial, evaluated on offset * <w_{trace_len*expansion}>.
+ * randomizers holds num_randomizers coefficients per column, column after column
+ * (randomizers[col*num_randomizers + k]) whatever the trace layout, on the host,
+ * or on the device with TVMC_TRACE_DEVICE.  num_randomizers = 0 with trace_offset = 1
+ * is tvmc_commit.  TVMC_RAND_TRUNCATE selects the truncating variant. */
+int tvmc_commit_randomized(const uint64_t* trace, size_t trace_len, size_t width, uint32_t expansion,
+                           uint64_t trace_offset, uint64_t offset, const uint64_t* randomizers,
+                           size_t num_randomizers, uint32_t flags, void* stream, tvmc_commitment** out);
 /* Wait for the commitment and copy its root (5 words) to host memory. */
 int tvmc_commitment_root(tvmc_commitment* c, uint64_t* root);
 int tvmc_commitment_sync(tvmc_commitment* c);

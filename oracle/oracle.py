@@ -64,6 +64,9 @@ class Oracle:
         L.tvmo_auth_structure_indices.argtypes = [ctypes.c_size_t, _szp, ctypes.c_size_t, _szp,
                                                   ctypes.c_size_t]
         L.tvmo_merkle_verify.argtypes = [_u64p, ctypes.c_size_t, _u64p, _u64p, ctypes.c_size_t]
+        L.tvmo_lde_randomized_column.argtypes = [_u64p, ctypes.c_size_t, _u64p, ctypes.c_size_t, _u64p,
+                                                 ctypes.c_size_t, ctypes.c_uint64, ctypes.c_uint64,
+                                                 ctypes.c_int]
 
     # field
     def mul(self, a, b): return self.L.tvmo_mul(a, b)
@@ -86,6 +89,21 @@ class Oracle:
         out = np.empty((w, n * expansion), dtype=np.uint64)
         if self.L.tvmo_lde_table(_ptr(t), n, w, _ptr(out), n * expansion, offset) != 0:
             raise ValueError("bad LDE size")
+        return out
+
+    def lde_randomized(self, trace_cm, rnd_cm, expansion: int = 4, offset: int = 7, trace_offset: int = 1,
+                       truncate: bool = False) -> np.ndarray:
+        """Randomized LDE of column-major (width, n) with randomizers (width, R)."""
+        t = np.ascontiguousarray(trace_cm, dtype=np.uint64)
+        w, n = t.shape
+        r = np.ascontiguousarray(rnd_cm, dtype=np.uint64).reshape(w, -1)
+        R = r.shape[1]
+        rr = r if R else np.zeros((w, 1), dtype=np.uint64)
+        out = np.empty((w, n * expansion), dtype=np.uint64)
+        for c in range(w):
+            if self.L.tvmo_lde_randomized_column(_ptr(t[c]), n, _ptr(rr[c]), R, _ptr(out[c]), n * expansion,
+                                                 trace_offset, offset, int(truncate)) != 0:
+                raise ValueError("bad LDE size")
         return out
 
     def permutation(self, state) -> np.ndarray:
@@ -188,6 +206,13 @@ class RefLib:
                                           ctypes.c_size_t]
         L.tvmr_commit.argtypes = [_u64p, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t,
                                   ctypes.c_uint64, _u64p, _u64p]
+        L.tvmr_lde_randomized.argtypes = [_u64p, ctypes.c_size_t, ctypes.c_size_t, _u64p, ctypes.c_size_t,
+                                          _u64p, ctypes.c_size_t, ctypes.c_uint64, ctypes.c_uint64]
+        L.tvmr_lde_randomized_xfe.argtypes = [_u64p, ctypes.c_size_t, ctypes.c_size_t, _u64p,
+                                              ctypes.c_size_t, ctypes.c_int, _u64p, ctypes.c_size_t,
+                                              ctypes.c_uint64, ctypes.c_uint64]
+        L.tvmr_lde_table_root.argtypes = [_u64p, ctypes.c_size_t, ctypes.c_size_t, _u64p, ctypes.c_size_t,
+                                          ctypes.c_size_t, ctypes.c_uint64, ctypes.c_uint64, _u64p]
         L.tvmr_max_threads.restype = ctypes.c_int
         L.tvmr_set_threads.argtypes = [ctypes.c_int]
 
@@ -227,6 +252,41 @@ class RefLib:
         out = np.empty((w, n * expansion), dtype=np.uint64)
         self.L.tvmr_lde_table(_ptr(t), n, w, _ptr(out), n * expansion, offset)
         return out
+
+    def lde_randomized(self, trace_cm, rnd_cm, expansion=4, offset=7, trace_offset=1):
+        t = np.ascontiguousarray(trace_cm, dtype=np.uint64)
+        w, n = t.shape
+        r = np.ascontiguousarray(rnd_cm, dtype=np.uint64).reshape(w, -1)
+        rr = r if r.size else np.zeros((w, 1), dtype=np.uint64)
+        out = np.empty((w, n * expansion), dtype=np.uint64)
+        self.L.tvmr_lde_randomized(_ptr(t), n, w, _ptr(rr), r.shape[1], _ptr(out), n * expansion,
+                                   trace_offset, offset)
+        return out
+
+    def lde_randomized_xfe(self, trace_x, rnd, expansion=4, offset=7, trace_offset=1):
+        """XFE columns (width, n, 3); rnd (width, R) base-field or (width, R, 3) XFE randomizers."""
+        t = np.ascontiguousarray(trace_x, dtype=np.uint64)
+        w, n, _ = t.shape
+        r = np.ascontiguousarray(rnd, dtype=np.uint64)
+        xr = int(r.ndim == 3)
+        R = r.shape[1]
+        rr = r if r.size else np.zeros(3, dtype=np.uint64)
+        out = np.empty((w, n * expansion, 3), dtype=np.uint64)
+        self.L.tvmr_lde_randomized_xfe(_ptr(t), n, w, _ptr(rr), R, xr, _ptr(out), n * expansion,
+                                       trace_offset, offset)
+        return out
+
+    def lde_table_root(self, rows_rm, rnd_cm, expansion=4, offset=7, trace_offset=1):
+        """LDETable::compute_lde_and_merkle of a row-major (n, width) table."""
+        t = np.ascontiguousarray(rows_rm, dtype=np.uint64)
+        n, w = t.shape
+        r = np.ascontiguousarray(rnd_cm, dtype=np.uint64).reshape(w, -1)
+        rr = r if r.size else np.zeros(1, dtype=np.uint64)
+        root = np.zeros(5, dtype=np.uint64)
+        if self.L.tvmr_lde_table_root(_ptr(t), n, w, _ptr(rr), r.shape[1], n * expansion, trace_offset,
+                                      offset, _ptr(root)) != 0:
+            raise ValueError("LDETable::compute_lde_and_merkle threw")
+        return root
 
     def hash_rows_cm(self, table_cm, r0=0, r1=None):
         t = np.ascontiguousarray(table_cm, dtype=np.uint64)

@@ -2,7 +2,7 @@
 //
 // Built by oracle/Makefile into oracle/_ref/libtvm_ref.so from the unchanged
 // reference files src/ntt/ntt.cpp, src/types/{b_field_element,x_field_element,digest}.cpp,
-// src/hash/tip5.cpp and src/merkle/merkle_tree.cpp.  It exposes a C ABI so
+// src/hash/tip5.cpp, src/merkle/merkle_tree.cpp and src/lde/{lde_randomized,lde_table}.cpp.  It exposes a C ABI so
 // that Python tests can (1) pin the C restatement in tvm_oracle.c against the
 // reference itself and (2) time the reference's CPU path as the benchmark's
 // CPU baseline.  The OpenMP loops over columns and rows are this harness's
@@ -16,6 +16,8 @@
 #include <omp.h>
 
 #include "hash/tip5.hpp"
+#include "lde/lde_randomized.hpp"
+#include "lde/lde_table.hpp"
 #include "merkle/merkle_tree.hpp"
 #include "ntt/ntt.hpp"
 #include "types/b_field_element.hpp"
@@ -161,6 +163,70 @@ int tvmr_commit(const uint64_t* trace, size_t n, size_t width, size_t L, uint64_
     try {
         MerkleTree t(lv);
         put_digest(t.root(), root);
+    } catch (...) {
+        return -1;
+    }
+    return 0;
+}
+
+// RandomizedLDE::extend_column_with_randomizer (src/lde/lde_randomized.cpp:71-154)
+// on each column-major column: trace[c*n + i] -> out[c*L + j]; randomizer
+// coefficients rnd[c*R + k].
+void tvmr_lde_randomized(const uint64_t* trace, size_t n, size_t width, const uint64_t* rnd, size_t R,
+                         uint64_t* out, size_t L, uint64_t trace_offset, uint64_t offset) {
+    const ArithmeticDomain td = domain(n, trace_offset), qd = domain(L, offset);
+#pragma omp parallel for schedule(dynamic)
+    for (long c = 0; c < (long)width; c++) {
+        std::vector<BFieldElement> col(n), r(R);
+        for (size_t i = 0; i < n; i++) col[i] = BFieldElement(trace[c * n + i]);
+        for (size_t k = 0; k < R; k++) r[k] = BFieldElement(rnd[c * R + k]);
+        auto e = RandomizedLDE::extend_column_with_randomizer(col, td, qd, r);
+        for (size_t j = 0; j < L; j++) out[c * L + j] = e[j].value();
+    }
+}
+
+// RandomizedLDE::extend_xfield_column_with_randomizer (xfe_rnd = 0, base-field
+// randomizer rnd[c*R + k]) and extend_xfield_column_with_xfield_randomizer
+// (xfe_rnd = 1, rnd[(c*R + k)*3 + limb]) on XFE columns trace[(c*n + i)*3 + limb];
+// out[(c*L + j)*3 + limb].
+void tvmr_lde_randomized_xfe(const uint64_t* trace, size_t n, size_t width, const uint64_t* rnd, size_t R,
+                             int xfe_rnd, uint64_t* out, size_t L, uint64_t trace_offset, uint64_t offset) {
+    const ArithmeticDomain td = domain(n, trace_offset), qd = domain(L, offset);
+    auto xfe = [](const uint64_t* v) {
+        return XFieldElement(BFieldElement(v[0]), BFieldElement(v[1]), BFieldElement(v[2]));
+    };
+#pragma omp parallel for schedule(dynamic)
+    for (long c = 0; c < (long)width; c++) {
+        std::vector<XFieldElement> col(n);
+        for (size_t i = 0; i < n; i++) col[i] = xfe(trace + 3 * (c * n + i));
+        std::vector<XFieldElement> e;
+        if (xfe_rnd) {
+            std::vector<XFieldElement> r(R);
+            for (size_t k = 0; k < R; k++) r[k] = xfe(rnd + 3 * (c * R + k));
+            e = RandomizedLDE::extend_xfield_column_with_xfield_randomizer(col, td, qd, r);
+        } else {
+            std::vector<BFieldElement> r(R);
+            for (size_t k = 0; k < R; k++) r[k] = BFieldElement(rnd[c * R + k]);
+            e = RandomizedLDE::extend_xfield_column_with_randomizer(col, td, qd, r);
+        }
+        for (size_t j = 0; j < L; j++)
+            for (int l = 0; l < 3; l++) out[3 * (c * L + j) + l] = e[j].coeff(l).value();
+    }
+}
+
+// LDETable::compute_lde_and_merkle (src/lde/lde_table.cpp:88-101) on a
+// row-major table rows[i*width + c] with randomizers rnd[c*R + k]; writes the
+// root.  Returns 0, or -1 when the reference throws.
+int tvmr_lde_table_root(const uint64_t* rows, size_t n, size_t width, const uint64_t* rnd, size_t R, size_t L,
+                        uint64_t trace_offset, uint64_t offset, uint64_t* root) {
+    std::vector<std::vector<BFieldElement>> t(n, std::vector<BFieldElement>(width));
+    for (size_t i = 0; i < n; i++)
+        for (size_t c = 0; c < width; c++) t[i][c] = BFieldElement(rows[i * width + c]);
+    std::vector<std::vector<BFieldElement>> r(width, std::vector<BFieldElement>(R));
+    for (size_t c = 0; c < width; c++)
+        for (size_t k = 0; k < R; k++) r[c][k] = BFieldElement(rnd[c * R + k]);
+    try {
+        put_digest(LDETable::compute_lde_and_merkle(t, domain(n, trace_offset), domain(L, offset), r), root);
     } catch (...) {
         return -1;
     }

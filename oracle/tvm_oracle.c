@@ -12,6 +12,9 @@
  *   NTT forward / inverse   src/ntt/ntt.cpp:8-86   (radix-2 DIT after bit reversal)
  *   evaluate_on_coset       src/ntt/ntt.cpp:94-117
  *   LDE::extend_column      src/ntt/ntt.cpp:121-131
+ *   RandomizedLDE           src/lde/lde_randomized.cpp:10-68 (zerofier * randomizer),
+ *                           :71-154 (extend_column_with_randomizer, incl. chunked
+ *                           evaluation), :178-277 (XFE variants: truncation to L)
  *   Tip5 permutation        src/hash/tip5.cpp:92-203
  *   Tip5::hash_varlen       src/hash/tip5.cpp:246-282
  *   Tip5::hash_10/hash_pair src/hash/tip5.cpp:224-297
@@ -175,6 +178,47 @@ int tvmo_lde_table(const uint64_t* trace, size_t n, size_t width, uint64_t* out,
     return 0;
 }
 
+/* RandomizedLDE::extend_column_with_randomizer: interpolant on the trace coset
+ * t * <omega_n> (inverse NTT, then c_i * t^-i), plus the zerofier times the
+ * randomizer, (x^n - t^n) * r(x), evaluated on o * <omega_L>.  A polynomial
+ * longer than L is evaluated chunk by chunk, chunk k scaled by o^(kL), as the
+ * reference does (truncate = 0); truncate = 1 drops every coefficient of
+ * degree >= L first, as the reference's XFieldElement variants do. */
+int tvmo_lde_randomized_column(const uint64_t* trace, size_t n, const uint64_t* r, size_t R, uint64_t* out,
+                               size_t L, uint64_t t, uint64_t o, int truncate) {
+    if (ilog2_exact(n) < 0 || ilog2_exact(L) < 0) return -1;
+    size_t len = R ? n + R : n;
+    uint64_t* p = (uint64_t*)calloc(len, sizeof(uint64_t));
+    uint64_t* ev = (uint64_t*)malloc(L * sizeof(uint64_t));
+    if (!p || !ev) {
+        free(p), free(ev);
+        return -2;
+    }
+    memcpy(p, trace, n * sizeof(uint64_t));
+    tvmo_ntt_inverse(p, n);
+    uint64_t ti = tvmo_inverse(gl_canon(t)), s = 1;
+    for (size_t i = 0; i < n; i++) {
+        p[i] = tvmo_mul(p[i], s);
+        s = tvmo_mul(s, ti);
+    }
+    uint64_t tn = tvmo_pow(gl_canon(t), n);
+    for (size_t k = 0; k < R; k++) {
+        uint64_t rk = gl_canon(r[k]);
+        p[k] = tvmo_sub(p[k], tvmo_mul(tn, rk));
+        p[n + k] = tvmo_add(p[n + k], rk);
+    }
+    if (truncate && len > L) len = L;
+    memset(out, 0, L * sizeof(uint64_t));
+    for (size_t c0 = 0; c0 < len; c0 += L) {
+        size_t m = len - c0 < L ? len - c0 : L;
+        tvmo_evaluate_on_coset(p + c0, m, ev, L, o);
+        uint64_t sc = tvmo_pow(gl_canon(o), c0);
+        for (size_t j = 0; j < L; j++) out[j] = tvmo_add(out[j], tvmo_mul(ev[j], sc));
+    }
+    free(p), free(ev);
+    return 0;
+}
+
 /* ----------------------------------------------------------------- Tip5 -- */
 
 #define T5_STATE 16
@@ -231,6 +275,14 @@ static uint64_t t5_montyred(uint64_t hi, uint64_t lo) {
     uint64_t r = hi - b;
     if (hi < b) r -= GL_EPS;
     return r;
+}
+
+/* The parameter tables above, for checking a product's exported copies. */
+void tvmo_tip5_parameters(uint8_t lookup[256], uint64_t mds[16], uint64_t rc[80]) {
+    t5_init();
+    memcpy(lookup, t5_lookup, 256);
+    memcpy(mds, t5_mds_col, sizeof t5_mds_col);
+    memcpy(rc, t5_rc, sizeof t5_rc);
 }
 
 /* split_and_lookup (tip5.cpp:119-145): to Montgomery form, byte-wise S-box,

@@ -7,8 +7,8 @@ from the reference's unchanged C++ sources first):
 
 Every array written here is an output of the reference prover's CPU functions
 (NTT::forward/inverse, LDE::extend_column, Tip5::permutation/hash_varlen/
-hash_pair, MerkleTree and its authentication paths/structure) on seeded
-inputs.  Tests compare both the CPU oracle and the CUDA path against them.
+hash_pair, MerkleTree and its authentication paths/structure, the randomized
+LDE of RandomizedLDE and LDETable::compute_lde_and_merkle) on seeded inputs.  Tests compare both the CPU oracle and the CUDA path against them.
 """
 import os
 import sys
@@ -69,6 +69,32 @@ def main():
         struct = r.auth_structure(leaves, sidx)
         np.savez(os.path.join(HERE, f"{name}.npz"), trace=trace, lde=lde, leaves=leaves, nodes=nodes,
                  root=nodes[1], path_idx=idx, paths=paths, struct_idx=sidx, struct=struct)
+
+    # Randomized (zero-knowledge) LDE: base-field columns, XFE columns with base
+    # or XFE randomizers, and the LDETable root.  Cases cover R = 0, N = 1, a
+    # trace offset != 1, polynomials longer than the LDE (chunked evaluation for
+    # base columns, truncation for XFE columns) and R = 98, the reference's
+    # default number of trace randomizers (src/stark.cpp:440-446).
+    rl = {}
+    for i, (n, R, E, t, o) in enumerate([(1, 0, 4, 1, 7), (1, 5, 4, 1, 7), (2, 3, 2, 3, 7), (4, 20, 2, 11, 7),
+                                         (8, 3, 4, 5, 7), (16, 0, 4, 3, 7), (64, 98, 4, 1, 7),
+                                         (256, 98, 8, 1, 7), (32, 98, 4, 1, 7), (128, 7, 2, 13, 5)]):
+        trace = rng.integers(0, P, (3, n), dtype=np.uint64)
+        rnd = rng.integers(0, P, (3, R), dtype=np.uint64)
+        rl[f"b{i}_meta"] = np.array([n, R, E, t, o], dtype=np.uint64)
+        rl[f"b{i}_trace"], rl[f"b{i}_rnd"] = trace, rnd
+        rl[f"b{i}_out"] = r.lde_randomized(trace, rnd, E, o, t)
+    for i, (n, R, E, t, xr) in enumerate([(4, 9, 2, 1, 0), (4, 9, 2, 1, 1), (32, 98, 4, 1, 0), (16, 5, 4, 3, 1)]):
+        trace = rng.integers(0, P, (2, n, 3), dtype=np.uint64)
+        rnd = rng.integers(0, P, (2, R, 3) if xr else (2, R), dtype=np.uint64)
+        rl[f"x{i}_meta"] = np.array([n, R, E, t, 7, xr], dtype=np.uint64)
+        rl[f"x{i}_trace"], rl[f"x{i}_rnd"] = trace, rnd
+        rl[f"x{i}_out"] = r.lde_randomized_xfe(trace, rnd, E, 7, t)
+    rows = rng.integers(0, P, (64, 23), dtype=np.uint64)
+    rnd = rng.integers(0, P, (23, 98), dtype=np.uint64)
+    rl["table_rows"], rl["table_rnd"] = rows, rnd
+    rl["table_root"] = r.lde_table_root(rows, rnd, 4, 7, 1)
+    np.savez(os.path.join(HERE, "lde_randomized.npz"), **rl)
     print("golden fixtures written to", HERE)
 
 

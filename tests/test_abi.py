@@ -75,3 +75,17 @@ def test_auth_structure_indices_match_oracle(oracle):
         tvmc.auth_structure_indices(8, [8])
     with pytest.raises(tvmc.InvalidArgument):
         tvmc.auth_structure_indices(6, [1])
+
+
+def test_tip5_parameters_match_oracle(oracle):
+    """The Tip5 tables the library exports (for the C++ Tip5 statics) equal the
+    oracle's, whose permutation is pinned by the upstream known-answer tests."""
+    import tvmc
+    lk, mds, rc = tvmc.tip5_parameters()
+    olk = np.zeros(256, np.uint8)
+    omds = np.zeros(16, np.uint64)
+    orc = np.zeros(80, np.uint64)
+    oracle.L.tvmo_tip5_parameters(olk.ctypes.data_as(ctypes.c_void_p), omds.ctypes.data_as(ctypes.c_void_p),
+                                  orc.ctypes.data_as(ctypes.c_void_p))
+    assert (lk == olk).all() and (mds == omds).all() and (rc == orc).all()
+    assert sorted(lk.tolist()) == list(range(256))  # a permutation of the bytes

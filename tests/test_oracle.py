@@ -127,3 +127,26 @@ def test_oracle_matches_reference_build(oracle):
     leaves = oracle.hash_rows_cm(lde)
     assert (leaves == r.hash_rows_cm(lde)).all()
     assert (oracle.merkle(leaves)[1:] == r.merkle(leaves)[1:]).all()
+
+
+def test_lde_randomized_golden(oracle):
+    """The oracle's randomized LDE equals the reference's RandomizedLDE outputs."""
+    g = golden("lde_randomized.npz")
+    for k in [k for k in g.files if k.endswith("_meta")]:
+        p = k[:-5]
+        if p.startswith("b"):
+            n, R, E, t, o = (int(v) for v in g[k])
+            got = oracle.lde_randomized(g[p + "_trace"], g[p + "_rnd"], E, o, t)
+        else:
+            n, R, E, t, o, xr = (int(v) for v in g[k])
+            tr, rnd = g[p + "_trace"], g[p + "_rnd"]
+            limbs = []
+            for l in range(3):
+                rl = rnd[:, :, l] if xr else (rnd if l == 0 else np.zeros_like(rnd))
+                limbs.append(oracle.lde_randomized(tr[:, :, l], rl, E, o, t, truncate=True))
+            got = np.stack(limbs, -1)
+        assert (got == g[p + "_out"]).all(), p
+    # LDETable::compute_lde_and_merkle root
+    rows, rnd = g["table_rows"], g["table_rnd"]
+    lde = oracle.lde_randomized(np.ascontiguousarray(rows.T), rnd, 4, 7, 1)
+    assert (oracle.merkle(oracle.hash_rows_cm(lde))[1] == g["table_root"]).all()

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "internal.cuh"
+#include "tip5_params.h"
 #include "tvmc.h"
 
 using namespace tvmc;
@@ -205,15 +206,52 @@ size_t lde_chunk_cols(int logn, int le, size_t width) {
     return std::min(width ? width : size_t(1), lim);
 }
 
+// Randomizer addends of one table on the device, [col][coset][rm] (launch_rand_addend).
+struct RandAdd {
+    const uint64_t* add = nullptr;
+    int rm = 0;
+    int le = 0;
+    const uint64_t* cols(size_t c0) const { return rm ? add + c0 * ((size_t)rm << le) : nullptr; }
+};
+
+// Enqueues the addends of `width` columns of R randomizer coefficients each
+// (device r[col*R + k]) on st; *buf (pool memory on st) is the caller's to free.
+int build_rand_add(const uint64_t* d_r, size_t R, size_t width, int logn, int le, uint64_t t, uint64_t o,
+                   bool truncate, cudaStream_t st, uint64_t** buf, RandAdd* ra) {
+    *buf = nullptr;
+    *ra = RandAdd{};
+    if (R == 0 || width == 0) return TVMC_OK;
+    const int rm = rand_rows(logn, R);
+    const size_t N = size_t(1) << logn, L = N << le;
+    CK(cudaMallocAsync((void**)buf, width * ((size_t)rm << le) * 8, st));
+    const uint64_t tc = t % P, oc = o % P;
+    const uint64_t qlen = truncate ? std::min<uint64_t>(N + R, L) : N + R;
+    cudaError_t e = launch_rand_addend(d_r, R, width, logn, le, tc, hpow(tc, N), hpow(oc, N), root_of_unity(le),
+                                       qlen, *buf, st);
+    if (e != cudaSuccess) {
+        cudaFreeAsync(*buf, st);
+        *buf = nullptr;
+        return cuda_fail(e, "randomizer addends");
+    }
+    ra->add = *buf;
+    ra->rm = rm;
+    ra->le = le;
+    return TVMC_OK;
+}
+
+// Coset offset of the LDE plan for trace offset t and evaluation offset o: o / t.
+uint64_t plan_offset(uint64_t t, uint64_t o) { return hmul(o % P, hinv(t % P)); }
+
 int run_lde(const LdePlan& pl, const uint64_t* d_tr, uint64_t tld, uint64_t* d_out, uint64_t old, size_t width,
-            cudaStream_t st) {
+            cudaStream_t st, const RandAdd& ra = RandAdd{}) {
     size_t chunk = lde_chunk_cols(pl.logn, pl.log_exp, width);
     size_t sw = lde_scratch_words(pl.logn, pl.log_exp, chunk);
     uint64_t* scratch = nullptr;
     if (sw) CK(cudaMallocAsync((void**)&scratch, sw * 8, st));
     for (size_t c0 = 0; c0 < width; c0 += chunk) {
         size_t nc = std::min(chunk, width - c0);
-        cudaError_t e = launch_lde(pl, d_tr + c0 * tld, tld, d_out + c0 * old, old, nc, scratch, st);
+        cudaError_t e =
+            launch_lde(pl, d_tr + c0 * tld, tld, d_out + c0 * old, old, nc, scratch, st, ra.cols(c0), ra.rm);
         if (e != cudaSuccess) {
             if (scratch) cudaFreeAsync(scratch, st);
             return cuda_fail(e, "launch_lde");
@@ -245,7 +283,7 @@ int copy_stream(cudaStream_t* out) {
 // device buffers: the copy stream uploads chunk k+1 while `st` runs the LDE of
 // chunk k.  Returns after enqueueing; `st` is ordered after every copy.
 int upload_lde_pipelined(const LdePlan& pl, const uint64_t* h_trace, size_t n, size_t width, uint64_t* d_out,
-                         size_t L, cudaStream_t st) {
+                         size_t L, cudaStream_t st, const RandAdd& ra = RandAdd{}) {
     cudaStream_t cs = nullptr;
     int rc = copy_stream(&cs);
     if (rc) return rc;
@@ -273,7 +311,7 @@ int upload_lde_pipelined(const LdePlan& pl, const uint64_t* h_trace, size_t n, s
             e = cudaMemcpyAsync(stage[b], h_trace + c0 * n, nc * n * 8, cudaMemcpyHostToDevice, cs);
         if (e == cudaSuccess) e = cudaEventRecord(ready[b], cs);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(st, ready[b], 0);
-        if (e == cudaSuccess) e = launch_lde(pl, stage[b], n, d_out + c0 * L, L, nc, scratch, st);
+        if (e == cudaSuccess) e = launch_lde(pl, stage[b], n, d_out + c0 * L, L, nc, scratch, st, ra.cols(c0), ra.rm);
         if (e == cudaSuccess) e = cudaEventRecord(freed[b], st);
     }
     for (int b = 0; b < 2; b++) {
@@ -324,12 +362,49 @@ struct DBuf {
     cudaError_t alloc(size_t words) { return cudaMalloc((void**)&p, words ? words * 8 : 8); }
 };
 
+// Per-thread, per-device device buffer reused by the host-buffer entry points,
+// so frequent small calls (one permutation, one path) pay no cudaMalloc/cudaFree.
+// Requests above 2^24 words get a buffer of their own instead.
+struct HostScratch {
+    std::map<int, std::pair<uint64_t*, size_t>> buf;
+    ~HostScratch() {
+        for (auto& kv : buf)
+            if (kv.second.first) cudaFree(kv.second.first);
+    }
+};
+thread_local HostScratch t_scratch;
+
+struct HostBuf {
+    uint64_t* p = nullptr;
+    DBuf own;
+};
+
+int host_buf(size_t words, HostBuf* hb) {
+    if (words > (size_t(1) << 24)) {
+        CK(hb->own.alloc(words));
+        hb->p = hb->own.p;
+        return TVMC_OK;
+    }
+    int dev;
+    CK(cudaGetDevice(&dev));
+    auto& b = t_scratch.buf[dev];
+    if (b.second < words) {
+        if (b.first) cudaFree(b.first);
+        b = {nullptr, 0};
+        const size_t cap = std::max(words, size_t(1) << 16);
+        CK(cudaMalloc((void**)&b.first, cap * 8));
+        b.second = cap;
+    }
+    hb->p = b.first;
+    return TVMC_OK;
+}
+
 // TVMC_FRUGAL commit: the LDE is produced stripe by stripe (10-column aligned)
 // and each stripe is absorbed at once into the per-row sponge capacity state,
 // so only one stripe of LDE (plus 48 bytes of state per row) is ever resident.
 // Leaves go straight into the heap tree `nodes`, which the last stripe completes.
 int commit_frugal(const LdePlan& pl, const uint64_t* trace, bool dev, bool rm, size_t n, size_t width, size_t L,
-                  uint64_t* nodes, cudaStream_t st, cudaEvent_t* prof) {
+                  uint64_t* nodes, cudaStream_t st, cudaEvent_t* prof, const RandAdd& ra) {
     const size_t NW = n * width;
     const uint64_t* src = trace;
     uint64_t *up = nullptr, *cm = nullptr, *cap = nullptr, *stripe = nullptr, *scratch = nullptr;
@@ -362,7 +437,7 @@ int commit_frugal(const LdePlan& pl, const uint64_t* trace, bool dev, bool rm, s
         const bool last = c0 + nc == width;
         for (size_t k = 0; k < nc && e == cudaSuccess; k += chunk) {
             const size_t kc = std::min(chunk, nc - k);
-            e = launch_lde(pl, src + (c0 + k) * n, n, stripe + k * L, L, kc, scratch, st);
+            e = launch_lde(pl, src + (c0 + k) * n, n, stripe + k * L, L, kc, scratch, st, ra.cols(c0 + k), ra.rm);
         }
         if (e == cudaSuccess) e = launch_absorb_stripe(stripe, L, (uint32_t)nc, cap, first, last, nodes, st);
         first = false;
@@ -534,6 +609,31 @@ int tvmc_ntt_host(uint64_t* data, size_t n, size_t num_cols, int inverse) {
     return TVMC_OK;
 }
 
+int tvmc_evaluate_on_coset_gpu(const uint64_t* d_coeffs, size_t num_coeffs, size_t num_cols, uint64_t* d_out,
+                               size_t domain_len, uint64_t offset, void* stream) {
+    if (!is_pow2(domain_len)) return fail(TVMC_ERR_INVALID, "NTT size must be a power of 2 (got %zu)", domain_len);
+    if (log2u(domain_len) > MAX_LOG_NTT)
+        return fail(TVMC_ERR_UNSUPPORTED, "NTT size 2^%d exceeds 2^%d", log2u(domain_len), MAX_LOG_NTT);
+    if (num_cols == 0) return TVMC_OK;
+    cudaStream_t st = as_stream(stream);
+    CK(launch_coset_scale(d_coeffs, num_coeffs, num_coeffs, d_out, domain_len, num_cols, offset, st));
+    return ntt_impl(d_out, domain_len, num_cols, 0, st);
+}
+
+int tvmc_evaluate_on_coset_host(const uint64_t* coeffs, size_t num_coeffs, size_t num_cols, uint64_t* out,
+                                size_t domain_len, uint64_t offset) {
+    if (!is_pow2(domain_len)) return fail(TVMC_ERR_INVALID, "NTT size must be a power of 2 (got %zu)", domain_len);
+    if (num_cols == 0) return TVMC_OK;
+    HostBuf hb;
+    int rc = host_buf(num_cols * (num_coeffs + domain_len), &hb);
+    if (rc) return rc;
+    uint64_t *a = hb.p, *b = a + num_cols * num_coeffs;
+    if (num_coeffs) CK(cudaMemcpy(a, coeffs, 8 * num_cols * num_coeffs, cudaMemcpyHostToDevice));
+    if ((rc = tvmc_evaluate_on_coset_gpu(a, num_coeffs, num_cols, b, domain_len, offset, nullptr))) return rc;
+    CK(cudaMemcpy(out, b, 8 * num_cols * domain_len, cudaMemcpyDeviceToHost));
+    return TVMC_OK;
+}
+
 // ---------------------------------------------------------------- LDE
 
 int tvmc_lde_batch_gpu(const uint64_t* d_traces, size_t num_columns, size_t trace_len, uint64_t* d_extended,
@@ -560,6 +660,51 @@ int tvmc_lde_host(const uint64_t* traces, size_t num_columns, size_t trace_len, 
     CK(cudaMemcpy(a.p, traces, trace_len * num_columns * 8, cudaMemcpyHostToDevice));
     if ((rc = tvmc_lde_batch_gpu(a.p, num_columns, trace_len, b.p, extended_len, 1, extended_offset, nullptr)))
         return rc;
+    CK(cudaMemcpy(extended, b.p, extended_len * num_columns * 8, cudaMemcpyDeviceToHost));
+    return TVMC_OK;
+}
+
+int tvmc_lde_randomized_gpu(const uint64_t* d_traces, size_t num_columns, size_t trace_len,
+                            const uint64_t* d_randomizers, size_t num_randomizers, uint64_t* d_extended,
+                            size_t extended_len, uint64_t trace_offset, uint64_t extended_offset, uint32_t flags,
+                            void* stream) {
+    int logn, le;
+    int rc = check_lde_sizes(trace_len, extended_len, &logn, &le);
+    if (rc) return rc;
+    if (flags & ~(uint32_t)TVMC_RAND_TRUNCATE) return fail(TVMC_ERR_INVALID, "unknown flag bits 0x%x", flags);
+    if (trace_offset % P == 0) return fail(TVMC_ERR_INVALID, "trace offset must be nonzero mod p");
+    if (num_columns == 0) return TVMC_OK;
+    if (num_randomizers && !d_randomizers) return fail(TVMC_ERR_INVALID, "null randomizers");
+    cudaStream_t st = as_stream(stream);
+    LdePlan pl;
+    if ((rc = get_plan(logn, le, plan_offset(trace_offset, extended_offset), &pl))) return rc;
+    uint64_t* d_add = nullptr;
+    RandAdd ra;
+    rc = build_rand_add(d_randomizers, num_randomizers, num_columns, logn, le, trace_offset, extended_offset,
+                        flags & TVMC_RAND_TRUNCATE, st, &d_add, &ra);
+    if (rc) return rc;
+    rc = run_lde(pl, d_traces, trace_len, d_extended, extended_len, num_columns, st, ra);
+    if (d_add) cudaFreeAsync(d_add, st);
+    return rc;
+}
+
+int tvmc_lde_randomized_host(const uint64_t* traces, size_t num_columns, size_t trace_len,
+                             const uint64_t* randomizers, size_t num_randomizers, uint64_t* extended,
+                             size_t extended_len, uint64_t trace_offset, uint64_t extended_offset, uint32_t flags) {
+    int logn, le;
+    int rc = check_lde_sizes(trace_len, extended_len, &logn, &le);
+    if (rc) return rc;
+    if (num_columns == 0) return TVMC_OK;
+    if (num_randomizers && !randomizers) return fail(TVMC_ERR_INVALID, "null randomizers");
+    DBuf a, b, r;
+    CK(a.alloc(trace_len * num_columns));
+    CK(b.alloc(extended_len * num_columns));
+    CK(r.alloc(num_randomizers * num_columns));
+    CK(cudaMemcpy(a.p, traces, trace_len * num_columns * 8, cudaMemcpyHostToDevice));
+    if (num_randomizers) CK(cudaMemcpy(r.p, randomizers, num_randomizers * num_columns * 8, cudaMemcpyHostToDevice));
+    rc = tvmc_lde_randomized_gpu(a.p, num_columns, trace_len, r.p, num_randomizers, b.p, extended_len, trace_offset,
+                                 extended_offset, flags, nullptr);
+    if (rc) return rc;
     CK(cudaMemcpy(extended, b.p, extended_len * num_columns * 8, cudaMemcpyDeviceToHost));
     return TVMC_OK;
 }
@@ -597,14 +742,14 @@ int tvmc_hash_pairs_gpu(const uint64_t* d_left, const uint64_t* d_right, uint64_
 
 int tvmc_hash_pairs_host(const uint64_t* left, const uint64_t* right, uint64_t* out, size_t count) {
     if (count == 0) return TVMC_OK;
-    DBuf a, b, c;
-    CK(a.alloc(5 * count));
-    CK(b.alloc(5 * count));
-    CK(c.alloc(5 * count));
-    CK(cudaMemcpy(a.p, left, 40 * count, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(b.p, right, 40 * count, cudaMemcpyHostToDevice));
-    CK(launch_hash_pairs(a.p, b.p, c.p, count, nullptr));
-    CK(cudaMemcpy(out, c.p, 40 * count, cudaMemcpyDeviceToHost));
+    HostBuf hb;
+    int rc = host_buf(15 * count, &hb);
+    if (rc) return rc;
+    uint64_t *a = hb.p, *b = a + 5 * count, *c = b + 5 * count;
+    CK(cudaMemcpy(a, left, 40 * count, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b, right, 40 * count, cudaMemcpyHostToDevice));
+    CK(launch_hash_pairs(a, b, c, count, nullptr));
+    CK(cudaMemcpy(out, c, 40 * count, cudaMemcpyDeviceToHost));
     return TVMC_OK;
 }
 
@@ -615,11 +760,41 @@ int tvmc_tip5_permutation_batch_gpu(uint64_t* d_states, size_t num_states, void*
 
 int tvmc_tip5_permutation_batch_host(uint64_t* states, size_t num_states) {
     if (num_states == 0) return TVMC_OK;
-    DBuf a;
-    CK(a.alloc(16 * num_states));
+    HostBuf a;
+    int rc = host_buf(16 * num_states, &a);
+    if (rc) return rc;
     CK(cudaMemcpy(a.p, states, 128 * num_states, cudaMemcpyHostToDevice));
     CK(launch_tip5_permutations(a.p, num_states, nullptr));
     CK(cudaMemcpy(states, a.p, 128 * num_states, cudaMemcpyDeviceToHost));
+    return TVMC_OK;
+}
+
+int tvmc_tip5_rounds_host(uint64_t* states, size_t num_states, uint32_t first_round, uint32_t num_rounds,
+                          uint64_t* trace) {
+    if (first_round > 5 || num_rounds > 5 - first_round)
+        return fail(TVMC_ERR_INVALID, "rounds [%u, %u) outside [0, 5)", first_round, first_round + num_rounds);
+    if (num_states == 0 || num_rounds == 0) return TVMC_OK;
+    HostBuf a;
+    int rc = host_buf(16 * num_states * (1 + (trace ? num_rounds : 0)), &a);
+    if (rc) return rc;
+    uint64_t* d_trace = trace ? a.p + 16 * num_states : nullptr;
+    CK(cudaMemcpy(a.p, states, 128 * num_states, cudaMemcpyHostToDevice));
+    CK(launch_tip5_rounds(a.p, num_states, (int)first_round, (int)num_rounds, d_trace, nullptr));
+    CK(cudaMemcpy(states, a.p, 128 * num_states, cudaMemcpyDeviceToHost));
+    if (trace) CK(cudaMemcpy(trace, d_trace, 128 * num_states * num_rounds, cudaMemcpyDeviceToHost));
+    return TVMC_OK;
+}
+
+int tvmc_tip5_parameters(uint8_t* lookup_table, uint64_t* mds_first_column, uint64_t* round_constants) {
+    static const uint64_t rc[80] = {TVMC_T5_ROUND_CONSTANTS};
+    static const uint64_t mds[16] = {TVMC_T5_MDS_FIRST_COLUMN};
+    if (lookup_table)
+        for (uint32_t i = 0; i < 256; i++) {
+            const uint32_t x = i + 1;  // offset Fermat cube map: (i + 1)^3 - 1 mod 257
+            lookup_table[i] = (uint8_t)((x * x % 257 * x % 257 + 256) % 257);
+        }
+    if (mds_first_column) std::memcpy(mds_first_column, mds, sizeof mds);
+    if (round_constants) std::memcpy(round_constants, rc, sizeof rc);
     return TVMC_OK;
 }
 
@@ -646,6 +821,29 @@ int tvmc_merkle_root_gpu(const uint64_t* d_leaves, uint64_t* d_root, size_t num_
     return TVMC_OK;
 }
 
+int tvmc_merkle_root_from_paths_gpu(const size_t* d_leaf_idx, const uint64_t* d_leaves, const uint64_t* d_paths,
+                                    size_t count, size_t path_len, uint64_t* d_roots, void* stream) {
+    static_assert(sizeof(size_t) == sizeof(uint64_t), "64-bit size_t");
+    CK(launch_root_from_paths(reinterpret_cast<const uint64_t*>(d_leaf_idx), d_leaves, d_paths, count, path_len,
+                              d_roots, as_stream(stream)));
+    return TVMC_OK;
+}
+
+int tvmc_merkle_root_from_paths_host(const size_t* leaf_idx, const uint64_t* leaves, const uint64_t* paths,
+                                     size_t count, size_t path_len, uint64_t* roots) {
+    if (count == 0) return TVMC_OK;
+    HostBuf hb;
+    int rc = host_buf(count * (11 + 5 * path_len), &hb);
+    if (rc) return rc;
+    uint64_t *ix = hb.p, *lv = ix + count, *pp = lv + 5 * count, *rt = pp + 5 * count * path_len;
+    CK(cudaMemcpy(ix, leaf_idx, 8 * count, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(lv, leaves, 40 * count, cudaMemcpyHostToDevice));
+    if (path_len) CK(cudaMemcpy(pp, paths, 40 * count * path_len, cudaMemcpyHostToDevice));
+    CK(launch_root_from_paths(ix, lv, pp, count, path_len, rt, nullptr));
+    CK(cudaMemcpy(roots, rt, 40 * count, cudaMemcpyDeviceToHost));
+    return TVMC_OK;
+}
+
 int tvmc_merkle_tree_heap_host(const uint64_t* leaves, size_t num_leaves, uint64_t* nodes) {
     if (!is_pow2(num_leaves))
         return fail(TVMC_ERR_INVALID, "Number of leaves must be a power of 2 (got %zu)", num_leaves);
@@ -663,20 +861,28 @@ int tvmc_merkle_tree_heap_host(const uint64_t* leaves, size_t num_leaves, uint64
 
 int tvmc_commit(const uint64_t* trace, size_t trace_len, size_t width, uint32_t expansion, uint64_t offset,
                 uint32_t flags, void* stream, tvmc_commitment** out) {
+    return tvmc_commit_randomized(trace, trace_len, width, expansion, 1, offset, nullptr, 0, flags, stream, out);
+}
+
+int tvmc_commit_randomized(const uint64_t* trace, size_t trace_len, size_t width, uint32_t expansion,
+                           uint64_t trace_offset, uint64_t offset, const uint64_t* randomizers,
+                           size_t num_randomizers, uint32_t flags, void* stream, tvmc_commitment** out) {
     if (!out) return fail(TVMC_ERR_INVALID, "null output handle");
     *out = nullptr;
     if (!is_pow2(expansion) || expansion > 16)
         return fail(TVMC_ERR_INVALID, "expansion factor %u is not a power of 2 <= 16", expansion);
     if (flags & ~(TVMC_TRACE_DEVICE | TVMC_TRACE_ROW_MAJOR | TVMC_DISCARD_LDE | TVMC_SYNC | TVMC_PROFILE |
-                  TVMC_FRUGAL))
+                  TVMC_FRUGAL | TVMC_RAND_TRUNCATE))
         return fail(TVMC_ERR_INVALID, "unknown flag bits 0x%x", flags);
     int logn, le;
     int rc = check_lde_sizes(trace_len, trace_len * expansion, &logn, &le);
     if (rc) return rc;
     if (width && !trace) return fail(TVMC_ERR_INVALID, "null trace");
+    if (trace_offset % P == 0) return fail(TVMC_ERR_INVALID, "trace offset must be nonzero mod p");
+    if (width && num_randomizers && !randomizers) return fail(TVMC_ERR_INVALID, "null randomizers");
     cudaStream_t st = as_stream(stream);
     LdePlan pl;
-    if ((rc = get_plan(logn, le, offset, &pl))) return rc;
+    if ((rc = get_plan(logn, le, plan_offset(trace_offset, offset), &pl))) return rc;
 
     tvmc_commitment* c = new tvmc_commitment();
     CK(cudaGetDevice(&c->device));
@@ -700,6 +906,34 @@ int tvmc_commit(const uint64_t* trace, size_t trace_len, size_t width, uint32_t 
     }
     if (cudaMemsetAsync(c->d_nodes, 0, 40, st) != cudaSuccess) return bail(cuda_fail(cudaGetLastError(), "memset"));
 
+    // randomizer addends (column-major [col][k], on the trace's side of the bus)
+    const size_t R = width ? num_randomizers : 0;
+    uint64_t *d_rnd = nullptr, *d_add = nullptr;
+    RandAdd ra;
+    if (R) {
+        const uint64_t* src_r = randomizers;
+        if (!(flags & TVMC_TRACE_DEVICE)) {
+            if (cudaMallocAsync((void**)&d_rnd, width * R * 8, st) != cudaSuccess ||
+                cudaMemcpyAsync(d_rnd, randomizers, width * R * 8, cudaMemcpyHostToDevice, st) != cudaSuccess) {
+                if (d_rnd) cudaFreeAsync(d_rnd, st);
+                return bail(cuda_fail(cudaGetLastError(), "randomizer upload"));
+            }
+            src_r = d_rnd;
+        }
+        rc = build_rand_add(src_r, R, width, logn, le, trace_offset, offset, flags & TVMC_RAND_TRUNCATE, st, &d_add,
+                            &ra);
+        if (d_rnd) cudaFreeAsync(d_rnd, st);
+        if (rc) return bail(rc);
+    }
+    // frees the addends (stream-ordered) on every exit from here on
+    struct AddGuard {
+        uint64_t* p;
+        cudaStream_t s;
+        ~AddGuard() {
+            if (p) cudaFreeAsync(p, s);
+        }
+    } add_guard{d_add, st};
+
     const bool prof = flags & TVMC_PROFILE;
     if (prof) {
         for (auto& ev : c->prof)
@@ -708,13 +942,14 @@ int tvmc_commit(const uint64_t* trace, size_t trace_len, size_t width, uint32_t 
     }
     const bool dev = flags & TVMC_TRACE_DEVICE, rm = flags & TVMC_TRACE_ROW_MAJOR;
     if (frugal) {
-        rc = commit_frugal(pl, trace, dev, rm, trace_len, width, c->L, c->d_nodes, st, prof ? c->prof : nullptr);
+        rc = commit_frugal(pl, trace, dev, rm, trace_len, width, c->L, c->d_nodes, st, prof ? c->prof : nullptr,
+                           ra);
         if (rc) return bail(rc);
     } else if (width && !dev && !rm) {
         // host column-major trace: upload column chunks on a copy stream,
         // overlapping the LDE of the previous chunk
         if (prof) cudaEventRecord(c->prof[1], st);
-        rc = upload_lde_pipelined(pl, trace, trace_len, width, c->d_lde, c->L, st);
+        rc = upload_lde_pipelined(pl, trace, trace_len, width, c->d_lde, c->L, st, ra);
         if (rc) return bail(rc);
     } else if (width) {
         const uint64_t* d_src = trace;
@@ -737,7 +972,7 @@ int tvmc_commit(const uint64_t* trace, size_t trace_len, size_t width, uint32_t 
             return bail(cuda_fail(e, "trace upload"));
         }
         if (prof) cudaEventRecord(c->prof[1], st);
-        rc = run_lde(pl, d_src, trace_len, c->d_lde, c->L, width, st);
+        rc = run_lde(pl, d_src, trace_len, c->d_lde, c->L, width, st, ra);
         if (d_up) cudaFreeAsync(d_up, st);
         if (d_cm) cudaFreeAsync(d_cm, st);
         if (rc) return bail(rc);

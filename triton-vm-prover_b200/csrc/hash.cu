@@ -221,6 +221,58 @@ __global__ void __launch_bounds__(128) k_tip5_perm(uint64_t* __restrict__ states
     for (int k = 0; k < T5_STATE; k++) states[16 * i + k] = gl_canon(s[k]);
 }
 
+// Rounds [r0, r0 + nr) on each state; with `trace`, the state after each round
+// at trace[(i*nr + k)*16 + .].
+__global__ void __launch_bounds__(128) k_tip5_rounds(uint64_t* __restrict__ states, uint64_t count, int r0, int nr,
+                                                     uint64_t* __restrict__ trace) {
+    __shared__ uint32_t sbox[T5_SBOX_WORDS];
+    t5_sbox_init(sbox);
+    __syncthreads();
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    uint64_t s[T5_STATE];
+#pragma unroll
+    for (int k = 0; k < T5_STATE; k++) s[k] = states[16 * i + k];
+    for (int k = 0; k < nr; k++) {
+        t5_round(s, sbox + (threadIdx.x & 31), r0 + k);
+        if (trace) {
+#pragma unroll
+            for (int j = 0; j < T5_STATE; j++) trace[(i * nr + k) * 16 + j] = gl_canon(s[j]);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < T5_STATE; k++) states[16 * i + k] = gl_canon(s[k]);
+}
+
+// Root implied by leaf q and its authentication path (MerkleTree::verify,
+// src/merkle/merkle_tree.cpp:343-364): paths[(q*len + k)*5 + .] is the sibling
+// at height k; leaf index bit k says which side the running digest is on.
+__global__ void __launch_bounds__(128) k_root_from_paths(const uint64_t* __restrict__ idx,
+                                                         const uint64_t* __restrict__ leaves,
+                                                         const uint64_t* __restrict__ paths, uint64_t count,
+                                                         uint64_t len, uint64_t* __restrict__ roots) {
+    __shared__ uint32_t sbox[T5_SBOX_WORDS];
+    t5_sbox_init(sbox);
+    __syncthreads();
+    uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= count) return;
+    uint64_t cur[5], sib[5];
+#pragma unroll
+    for (int j = 0; j < 5; j++) cur[j] = gl_canon(leaves[5 * q + j]);
+    uint64_t at = idx[q];
+    for (uint64_t k = 0; k < len; k++) {
+#pragma unroll
+        for (int j = 0; j < 5; j++) sib[j] = gl_canon(paths[(q * len + k) * 5 + j]);
+        if (at & 1)
+            t5_hash_pair(sib, cur, cur, sbox + (threadIdx.x & 31));
+        else
+            t5_hash_pair(cur, sib, cur, sbox + (threadIdx.x & 31));
+        at >>= 1;
+    }
+#pragma unroll
+    for (int j = 0; j < 5; j++) roots[5 * q + j] = cur[j];
+}
+
 __global__ void k_gather_auth(const uint64_t* __restrict__ tree, uint64_t n, int layout, int height,
                               const uint64_t* __restrict__ idx, uint64_t count, uint64_t* __restrict__ out) {
     uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -326,6 +378,21 @@ cudaError_t launch_tip5_permutations(uint64_t* states, uint64_t count, cudaStrea
     if (count == 0) return cudaSuccess;
     count_launch();
     k_tip5_perm<<<grid_for(count, 128), 128, 0, st>>>(states, count);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tip5_rounds(uint64_t* states, uint64_t count, int r0, int nr, uint64_t* trace, cudaStream_t st) {
+    if (count == 0 || nr == 0) return cudaSuccess;
+    count_launch();
+    k_tip5_rounds<<<grid_for(count, 128), 128, 0, st>>>(states, count, r0, nr, trace);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_root_from_paths(const uint64_t* idx, const uint64_t* leaves, const uint64_t* paths, uint64_t count,
+                                   uint64_t len, uint64_t* roots, cudaStream_t st) {
+    if (count == 0) return cudaSuccess;
+    count_launch();
+    k_root_from_paths<<<grid_for(count, 128), 128, 0, st>>>(idx, leaves, paths, count, len, roots);
     return cudaGetLastError();
 }
 

@@ -56,6 +56,11 @@ cudaError_t launch_absorb_stripe(const uint64_t* stripe, uint64_t L, uint32_t nc
 cudaError_t launch_hash_pairs(const uint64_t* left, const uint64_t* right, uint64_t* out, uint64_t count,
                               cudaStream_t st);
 cudaError_t launch_tip5_permutations(uint64_t* states, uint64_t count, cudaStream_t st);
+// Tip5 rounds [r0, r0 + nr) of each state; trace (optional) gets the state after each round.
+cudaError_t launch_tip5_rounds(uint64_t* states, uint64_t count, int r0, int nr, uint64_t* trace, cudaStream_t st);
+// roots[q] = root implied by leaf digest leaves[q] at index idx[q] and its path of len siblings.
+cudaError_t launch_root_from_paths(const uint64_t* idx, const uint64_t* leaves, const uint64_t* paths, uint64_t count,
+                                   uint64_t len, uint64_t* roots, cudaStream_t st);
 // out[q*height + k] = sibling of the k-th ancestor of leaf idx[q] (k = 0 is the leaf's sibling).
 cudaError_t launch_gather_auth_paths(const uint64_t* tree, uint64_t n, int layout, const uint64_t* idx,
                                      uint64_t count, uint64_t* out, cudaStream_t st);
@@ -85,13 +90,30 @@ struct LdePlan {
 
 // Batched LDE of `cols` column-major columns: trace[c*tld + r] (r < N) ->
 // out[c*old + r] (r < E*N).  scratch must hold scratch_words_lde(...) words.
+// With rm > 0, add holds the randomizer addends of launch_rand_addend for
+// these columns ([col][coset][rm]); the plan's offset is then o / t.
 size_t lde_scratch_words(int logn, int log_exp, uint64_t cols);
 cudaError_t launch_lde(const LdePlan& pl, const uint64_t* trace, uint64_t tld, uint64_t* out, uint64_t old,
-                       uint64_t cols, uint64_t* scratch, cudaStream_t st);
+                       uint64_t cols, uint64_t* scratch, cudaStream_t st, const uint64_t* add = nullptr,
+                       int rm = 0);
+// Interpolant coefficients touched by R randomizer coefficients: min(N, R).
+inline int rand_rows(int logn, uint64_t R) {
+    return R < (1ull << logn) ? (int)R : (1 << logn);
+}
+// Randomizer addends for `cols` columns with R coefficients each (r[col*R + k]):
+// out[(col*E + c)*rm + i], rm = rand_rows(logn, R).  t = trace offset, tN = t^N,
+// oN = o^N for the evaluation offset o, wE = primitive E-th root of unity; the
+// product (x^N - t^N) r(x) is truncated to degree < qlen.
+cudaError_t launch_rand_addend(const uint64_t* r, uint64_t R, uint64_t cols, int logn, int le, uint64_t t,
+                               uint64_t tN, uint64_t oN, uint64_t wE, uint64_t qlen, uint64_t* out, cudaStream_t st);
 // Batched NTT in place on column-major data[c*ld + r], r < 2^logn.
 size_t ntt_scratch_words(int logn, uint64_t cols);
 cudaError_t launch_ntt(const LdePlan& pl, int inverse, uint64_t* data, uint64_t ld, uint64_t cols,
                        uint64_t* scratch, cudaStream_t st);
+// out[c*L + i] = in[c*ild + i] * o^i for i < min(n, L), 0 above (the coefficient
+// side of NTT::evaluate_on_coset); a forward NTT of length L finishes it.
+cudaError_t launch_coset_scale(const uint64_t* in, uint64_t ild, uint64_t n, uint64_t* out, uint64_t L, uint64_t cols,
+                               uint64_t o, cudaStream_t st);
 // Row-major (rows x cols, row stride rld) -> column-major (col stride cld).
 cudaError_t launch_transpose(const uint64_t* in, uint64_t rld, uint64_t* out, uint64_t cld, uint64_t rows,
                              uint64_t cols, cudaStream_t st);

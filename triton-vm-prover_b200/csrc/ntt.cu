@@ -293,7 +293,7 @@ __global__ void __launch_bounds__(NTT_THREADS) k_lde_small(const uint64_t* trace
                                                            uint64_t old, uint64_t cols, int lT, int le,
                                                            const uint64_t* tw12_i, const uint64_t* tw12_f,
                                                            const uint64_t* sc_lo, const uint64_t* sc_hi,
-                                                           int hi_len) {
+                                                           int hi_len, const uint64_t* add, int rm) {
     extern __shared__ uint64_t sm[];
     constexpr int n = 1 << LS;
     const int E = 1 << le;
@@ -314,7 +314,12 @@ __global__ void __launch_bounds__(NTT_THREADS) k_lde_small(const uint64_t* trace
         const uint64_t* lo = sc_lo + 4096 * c;
         const uint64_t* hi = sc_hi + hi_len * c;
         sub_dft<LS>(
-            s, lT, twf, [&](int k, int t) { return gl_mul_c(cf[spos(k, lT) + t], tw2(lo, hi, (uint32_t)k)); },
+            s, lT, twf,
+            [&](int k, int t) {
+                uint64_t x = cf[spos(k, lT) + t];
+                if (rm && k < rm && c0 + t < cols) x = gl_add_pc(x, add[((c0 + t) * E + c) * rm + k]);
+                return gl_mul_c(x, tw2(lo, hi, (uint32_t)k));
+            },
             [&](int q, int t, uint64_t v) {
                 if (c0 + t < cols) out[(c0 + t) * old + (uint64_t)q * E + c] = v;
             });
@@ -349,12 +354,13 @@ __global__ void __launch_bounds__(NTT_THREADS) k_lde_inv_a(const uint64_t* trace
 // K2: rows k2 in [k20, k20+T) of Y: inverse DFT_n1 -> coefficients c[n2*k1 + k2];
 // per coset: a = c * N^-1 s_c^i, forward DFT_n1 over k1, times w_N^(k2*q2),
 // Z_c[k2 + n2*q2].  Z holds E planes of N words per column: Z[(col*E + c)*N + .].
-template <int L1>
+template <int L1, bool RAND>
 __global__ void __launch_bounds__(NTT_THREADS) k_lde_mid(const uint64_t* Y, uint64_t yld, uint64_t* Z, int l2,
                                                          int lT, int le, const uint64_t* tw12_i,
                                                          const uint64_t* tw12_f, const uint64_t* wlo,
                                                          const uint64_t* whi, const uint64_t* sc_lo,
-                                                         const uint64_t* sc_hi, int hi_len) {
+                                                         const uint64_t* sc_hi, int hi_len, const uint64_t* add,
+                                                         int rm) {
     extern __shared__ uint64_t sm[];
     constexpr int n1 = 1 << L1;
     const int E = 1 << le;
@@ -380,7 +386,12 @@ __global__ void __launch_bounds__(NTT_THREADS) k_lde_mid(const uint64_t* Y, uint
         sub_dft<L1, true>(
             s, lT, twf,
             [&](int k, int t) {
-                return gl_mul_c(cf[spos(k, lT) + t], tw2(lo, hi, ((uint32_t)k << l2) + k20 + t));
+                uint64_t x = cf[spos(k, lT) + t];
+                const uint32_t i = ((uint32_t)k << l2) + k20 + t;
+                if constexpr (RAND) {
+                    if (i < (uint32_t)rm) x = gl_add_pc(x, add[(col * E + c) * rm + i]);
+                }
+                return gl_mul_c(x, tw2(lo, hi, i));
             },
             [](int, int, uint64_t) {});
         __syncthreads();
@@ -400,11 +411,12 @@ __global__ void __launch_bounds__(NTT_THREADS) k_lde_mid(const uint64_t* Y, uint
 // i = i1 + R2*i2 makes its first round take exactly that set (i1 = k), so the
 // coefficients stay in registers for all E cosets and only the forward's
 // second round goes through shared memory.
-template <int L1>
+template <int L1, bool RAND>
 __global__ void __launch_bounds__(128) k_lde_mid_reg(const uint64_t* Y, uint64_t yld, uint64_t* Z, int l2, int le,
                                                      const uint64_t* tw12_i, const uint64_t* tw12_f,
                                                      const uint64_t* wlo, const uint64_t* whi,
-                                                     const uint64_t* sc_lo, const uint64_t* sc_hi, int hi_len) {
+                                                     const uint64_t* sc_lo, const uint64_t* sc_hi, int hi_len,
+                                                     const uint64_t* add, int rm) {
     using PL = Plan<L1>;
     static_assert(PL::NR == 2, "two-round sizes only");
     constexpr int b1 = PL::b1, b2 = PL::b2, R1 = 1 << b1, R2 = 1 << b2;
@@ -458,7 +470,12 @@ __global__ void __launch_bounds__(128) k_lde_mid_reg(const uint64_t* Y, uint64_t
 #pragma unroll
             for (int k1 = 0; k1 < R1; k1++) {
                 const uint32_t ci = (uint32_t)kk + ((uint32_t)k1 << b2);
-                v[k1] = gl_mul_c(cf[k1], tw2(lo, hi, (ci << l2) + k20 + t));
+                const uint32_t i = (ci << l2) + k20 + t;
+                uint64_t x = cf[k1];
+                if constexpr (RAND) {
+                    if (i < (uint32_t)rm) x = gl_add_pc(x, add[(col * E + c) * rm + i]);
+                }
+                v[k1] = gl_mul_c(x, tw2(lo, hi, i));
             }
             reg_dft<L1, b1>(v, twf);
 #pragma unroll
@@ -494,11 +511,12 @@ __global__ void __launch_bounds__(128) k_lde_mid_reg(const uint64_t* Y, uint64_t
 // E forward transforms run through ONE rolled loop over (pass, round) around
 // a single register DFT body, so the kernel's code stays small enough for the
 // instruction cache.  Thread (t, ln) owns line ln of every round.
-template <int L1, int MINB>
+template <int L1, int MINB, bool RAND>
 __global__ void __launch_bounds__(128, MINB) k_lde_mid_sym(const uint64_t* Y, uint64_t yld, uint64_t* Z, int l2, int le,
                                                      const uint64_t* tw12_i, const uint64_t* tw12_f,
                                                      const uint64_t* wlo, const uint64_t* whi,
-                                                     const uint64_t* sc_lo, const uint64_t* sc_hi, int hi_len) {
+                                                     const uint64_t* sc_lo, const uint64_t* sc_hi, int hi_len,
+                                                     const uint64_t* add, int rm) {
     using PL = Plan<L1>;
     static_assert(PL::NR == 2 && PL::b1 == PL::b2, "square sizes only");
     constexpr int B = PL::b1, R = 1 << B;
@@ -534,7 +552,12 @@ __global__ void __launch_bounds__(128, MINB) k_lde_mid_sym(const uint64_t* Y, ui
 #pragma unroll
                     for (int k1 = 0; k1 < R; k1++) {
                         const uint32_t ci = (uint32_t)ln + ((uint32_t)k1 << B);
-                        v[k1] = gl_mul_c(cf[k1], tw2(lo, hi, (ci << l2) + k20 + t));
+                        const uint32_t i = (ci << l2) + k20 + t;
+                        uint64_t x = cf[k1];
+                        if constexpr (RAND) {
+                            if (i < (uint32_t)rm) x = gl_add_pc(x, add[(col * E + pass - 1) * rm + i]);
+                        }
+                        v[k1] = gl_mul_c(x, tw2(lo, hi, i));
                     }
                 }
             } else {  // round 2 of either: slots x + R*ln
@@ -595,6 +618,58 @@ __global__ void __launch_bounds__(NTT_THREADS) k_lde_fwd_b(const uint64_t* Z, ui
             return src[(uint64_t)c * N + ((uint64_t)t << L2) + k];
         },
         [&](int q, int u, uint64_t v) { dst[(((uint64_t)q << l1) * E) + u] = v; });
+}
+
+// N = 1: the interpolant is the constant trace value; coset c of the LDE is the
+// single point s_c, where the randomizer term contributes add[(col*E + c)*rm].
+__global__ void k_lde_one(const uint64_t* trace, uint64_t tld, uint64_t* out, uint64_t old, uint64_t total,
+                          int le, const uint64_t* add, int rm) {
+    const uint64_t idx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= total) return;
+    const uint64_t col = idx >> le, c = idx & ((1u << le) - 1);
+    uint64_t x = gl_canon(trace[col * tld]);
+    if (rm) x = gl_add_c(x, add[idx * rm]);
+    out[col * old + c] = x;
+}
+
+// Randomizer term of the zero-knowledge LDE, folded per coset into addends of
+// the first rm = min(N, R) interpolant coefficients.  Per column the extended
+// polynomial is a(x) + q(x) with q = (x^N - t^N) r(x), truncated to degree <
+// qlen.  On coset c of the evaluation domain, x^N equals z_c = o^N w_E^c, so
+// q(x) there equals sum_k z_c^k q_{i + kN} x^i (i < N).  The LDE kernels add
+// out[(col*E + c)*rm + i] = N t^i sum_k z_c^k q_{i+kN} to the raw (unscaled)
+// coefficient i before multiplying by N^-1 (s_c / t)^i.
+__global__ void k_rand_addend(const uint64_t* r, uint64_t R, uint64_t total, int logn, int le, int rm, uint64_t t,
+                              uint64_t tN, uint64_t oN, uint64_t wE, uint64_t qlen, uint64_t* out) {
+    const uint64_t N = 1ull << logn;
+    for (uint64_t idx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t i = idx % (uint64_t)rm, cc = idx / (uint64_t)rm;
+        const uint64_t c = cc & ((1u << le) - 1), col = cc >> le;
+        const uint64_t* rc = r + col * R;
+        const uint64_t zc = gl_mul_c(oN, gl_canon(gl_pow(wE, c)));
+        uint64_t acc = 0, zk = 1;
+        for (uint64_t j = i; j < qlen; j += N) {
+            uint64_t q = 0;
+            if (j < R) q = gl_sub_c(0, gl_mul_c(tN, gl_canon(rc[j])));
+            if (j >= N && j - N < R) q = gl_add_c(q, gl_canon(rc[j - N]));
+            acc = gl_add_c(acc, gl_mul_c(zk, q));
+            zk = gl_mul_c(zk, zc);
+        }
+        out[idx] = gl_mul_c(gl_mul_c(N % GL_P, gl_canon(gl_pow(t, i))), acc);
+    }
+}
+
+cudaError_t launch_rand_addend(const uint64_t* r, uint64_t R, uint64_t cols, int logn, int le, uint64_t t,
+                               uint64_t tN, uint64_t oN, uint64_t wE, uint64_t qlen, uint64_t* out, cudaStream_t st) {
+    const int rm = rand_rows(logn, R);
+    const uint64_t total = (cols << le) * (uint64_t)rm;
+    if (total == 0) return cudaSuccess;
+    const uint64_t blocks = (total + 255) / 256;
+    count_launch();
+    k_rand_addend<<<(unsigned)(blocks < 148 * 16 ? blocks : 148 * 16), 256, 0, st>>>(r, R, total, logn, le, rm, t,
+                                                                                   tN, oN, wE, qlen, out);
+    return cudaGetLastError();
 }
 
 // ------------------------------------------------------------------ helpers
@@ -693,19 +768,16 @@ size_t lde_scratch_words(int logn, int log_exp, uint64_t cols) {
 }
 
 cudaError_t launch_lde(const LdePlan& pl, const uint64_t* trace, uint64_t tld, uint64_t* out, uint64_t old,
-                       uint64_t cols, uint64_t* scratch, cudaStream_t st) {
+                       uint64_t cols, uint64_t* scratch, cudaStream_t st, const uint64_t* add, int rm) {
     const int l = pl.logn, le = pl.log_exp;
     const int hi_len = l > 12 ? (1 << (l - 12)) : 1;
     if (cols == 0) return cudaSuccess;
     if (l <= 11) {
         if (l == 0) {
-            // N = 1: every LDE row equals the single trace value (constant polynomial)
-            const int E = 1 << le;
-            cudaError_t e = cudaSuccess;
-            for (uint64_t c = 0; c < cols && e == cudaSuccess; c++)
-                for (int r = 0; r < E && e == cudaSuccess; r++)
-                    e = cudaMemcpyAsync(out + c * old + r, trace + c * tld, 8, cudaMemcpyDeviceToDevice, st);
-            return e;
+            const uint64_t total = cols << le;
+            count_launch();
+            k_lde_one<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(trace, tld, out, old, total, le, add, rm);
+            return cudaGetLastError();
         }
         const int lT = choose_lT(l, 10);
         const int T = 1 << lT;
@@ -715,7 +787,7 @@ cudaError_t launch_lde(const LdePlan& pl, const uint64_t* trace, uint64_t tld, u
             if (e != cudaSuccess) return e;
             count_launch();
             k_lde_small<LS><<<(unsigned)((cols + T - 1) / T), NTT_THREADS, smem, st>>>(
-                trace, tld, out, old, cols, lT, le, pl.tw12_i, pl.tw12_f, pl.sc_lo, pl.sc_hi, hi_len);
+                trace, tld, out, old, cols, lT, le, pl.tw12_i, pl.tw12_f, pl.sc_lo, pl.sc_hi, hi_len, add, rm);
             return cudaGetLastError();
         });
     }
@@ -731,6 +803,7 @@ cudaError_t launch_lde(const LdePlan& pl, const uint64_t* trace, uint64_t tld, u
     for (uint64_t c0 = 0; c0 < cols; c0 += 65535) {
         const unsigned nc = (unsigned)((cols - c0) < 65535 ? (cols - c0) : 65535);
         uint64_t* Z = scratch + (size_t)nc * N;
+        const uint64_t* addc = rm ? add + c0 * ((uint64_t)rm << le) : nullptr;
         cudaError_t e = dispatch_ls(l2, [&]<int L2>() -> cudaError_t {
             cudaError_t e2 = set_smem((const void*)k_lde_inv_a<L2>, smem1);
             if (e2 != cudaSuccess) return e2;
@@ -745,26 +818,33 @@ cudaError_t launch_lde(const LdePlan& pl, const uint64_t* trace, uint64_t tld, u
                 constexpr int lTr = 7 - Plan<L1>::b2;
                 const size_t smr = words_bytes(2 * (size_t)(1u << L1) + spad_words(1 << L1, lTr));
                 // register budget: 2 resident CTAs (no spills) or 3 (a few spills); tuning knob
-                auto kern = tuning_lde_mid_ctas() == 3 ? k_lde_mid_sym<L1, 3> : k_lde_mid_sym<L1, 2>;
+                // (the randomized variant runs at 2 CTAs per SM)
+                auto kern = rm ? k_lde_mid_sym<L1, 2, true>
+                               : (tuning_lde_mid_ctas() == 3 ? k_lde_mid_sym<L1, 3, false> : k_lde_mid_sym<L1, 2, false>);
                 cudaError_t e2 = set_smem((const void*)kern, smr);
                 if (e2 != cudaSuccess) return e2;
                 count_launch();
                 kern<<<dim3((1u << l2) >> lTr, nc), 128, smr, st>>>(
-                    Y, N, Z, l2, le, pl.tw12_i, pl.tw12_f, pl.wn_f_lo, pl.wn_f_hi, pl.sc_lo, pl.sc_hi, hi_len);
+                    Y, N, Z, l2, le, pl.tw12_i, pl.tw12_f, pl.wn_f_lo, pl.wn_f_hi, pl.sc_lo, pl.sc_hi, hi_len,
+                    addc, rm);
             } else if constexpr (Plan<L1>::NR == 2) {
                 constexpr int lTr = 7 - Plan<L1>::b2;
                 const size_t smr = words_bytes(2 * (size_t)(1u << L1) + spad_words(1 << L1, lTr));
-                cudaError_t e2 = set_smem((const void*)k_lde_mid_reg<L1>, smr);
+                auto kern = rm ? k_lde_mid_reg<L1, true> : k_lde_mid_reg<L1, false>;
+                cudaError_t e2 = set_smem((const void*)kern, smr);
                 if (e2 != cudaSuccess) return e2;
                 count_launch();
-                k_lde_mid_reg<L1><<<dim3((1u << l2) >> lTr, nc), 128, smr, st>>>(
-                    Y, N, Z, l2, le, pl.tw12_i, pl.tw12_f, pl.wn_f_lo, pl.wn_f_hi, pl.sc_lo, pl.sc_hi, hi_len);
+                kern<<<dim3((1u << l2) >> lTr, nc), 128, smr, st>>>(
+                    Y, N, Z, l2, le, pl.tw12_i, pl.tw12_f, pl.wn_f_lo, pl.wn_f_hi, pl.sc_lo, pl.sc_hi, hi_len,
+                    addc, rm);
             } else {
-                cudaError_t e2 = set_smem((const void*)k_lde_mid<L1>, smem2);
+                auto kern = rm ? k_lde_mid<L1, true> : k_lde_mid<L1, false>;
+                cudaError_t e2 = set_smem((const void*)kern, smem2);
                 if (e2 != cudaSuccess) return e2;
                 count_launch();
-                k_lde_mid<L1><<<dim3((1u << l2) >> lT2, nc), NTT_THREADS, smem2, st>>>(
-                    Y, N, Z, l2, lT2, le, pl.tw12_i, pl.tw12_f, pl.wn_f_lo, pl.wn_f_hi, pl.sc_lo, pl.sc_hi, hi_len);
+                kern<<<dim3((1u << l2) >> lT2, nc), NTT_THREADS, smem2, st>>>(
+                    Y, N, Z, l2, lT2, le, pl.tw12_i, pl.tw12_f, pl.wn_f_lo, pl.wn_f_hi, pl.sc_lo, pl.sc_hi, hi_len,
+                    addc, rm);
             }
             return cudaGetLastError();
         });
@@ -780,6 +860,33 @@ cudaError_t launch_lde(const LdePlan& pl, const uint64_t* trace, uint64_t tld, u
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
+}
+
+// ------------------------------------------------------------ coset scale
+
+// 16 consecutive coefficients per thread: one power, then running products.
+__global__ void k_coset_scale(const uint64_t* __restrict__ in, uint64_t ild, uint64_t n, uint64_t* __restrict__ out,
+                              uint64_t L, uint64_t cols, uint64_t o) {
+    const uint64_t per_col = (L + 15) / 16;
+    for (uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; g < cols * per_col;
+         g += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t c = g / per_col, i0 = (g - c * per_col) * 16;
+        uint64_t w = gl_canon(gl_pow(o, i0));
+        for (uint64_t i = i0; i < i0 + 16 && i < L; i++) {
+            out[c * L + i] = i < n ? gl_mul_c(gl_canon(in[c * ild + i]), w) : 0;
+            w = gl_mul_c(w, o);
+        }
+    }
+}
+
+cudaError_t launch_coset_scale(const uint64_t* in, uint64_t ild, uint64_t n, uint64_t* out, uint64_t L, uint64_t cols,
+                               uint64_t o, cudaStream_t st) {
+    const uint64_t work = cols * ((L + 15) / 16);
+    if (work == 0) return cudaSuccess;
+    const uint64_t blocks = (work + 255) / 256;
+    count_launch();
+    k_coset_scale<<<(unsigned)(blocks < 148 * 8 ? blocks : 148 * 8), 256, 0, st>>>(in, ild, n, out, L, cols, o % GL_P);
+    return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------- transpose

@@ -17,6 +17,7 @@
 #pragma once
 #include <cstdint>
 #include "field.cuh"
+#include "tip5_params.h"
 
 namespace tvmc {
 
@@ -24,30 +25,9 @@ constexpr int T5_STATE = 16;
 constexpr int T5_RATE = 10;
 constexpr int T5_ROUNDS = 5;
 
-// Round constants of Tip5 (published parameters; identical to
-// src/hash/tip5.cpp:33-79).  The MDS first column (tip5.cpp:27-30) is inlined
-// in t5_mds below.
-__device__ __constant__ uint64_t c_t5_rc[T5_ROUNDS * T5_STATE] = {
-    0xBD2A3DEB61AB60DEull, 0xEA7DF21AD9547ED2ull, 0x900B3677A1DE063Full, 0x1B46887E876C8677ull,
-    0xD364D977889CFB97ull, 0xDC8DFAC843699F02ull, 0x375C405D7190DB58ull, 0x27924006D2B0D4B1ull,
-    0x78DD1172D483CD38ull, 0x3346C66244882A56ull, 0xB0249B279F498AA5ull, 0x94CD51BE79338D4Dull,
-    0xB0E0DC7052C5B218ull, 0xF8DCC4D248ADAD95ull, 0x68E3C635FEC868B7ull, 0xD7D06B3FFB6B0D8Cull,
-    0xF3500DEA20EF032Aull, 0x4865BF175BBA5803ull, 0xD5F7FE3027287A27ull, 0xA57333F44E193412ull,
-    0x8726E153A977EAE2ull, 0x3014A98463FC191Bull, 0xBA145461AF39B212ull, 0x03AB70105933202Full,
-    0x3D90B7EEBFCF71E5ull, 0x386322B1CC520BFDull, 0x27C2C8DAF774F675ull, 0x4FCB83F50309BC6Aull,
-    0x5E6D5CE8275F3CB3ull, 0xECC2F6592C8F905Cull, 0x837F532461E609B4ull, 0xB2B1F6B95C92C93Cull,
-    0xC0027AF556411DC1ull, 0x16E18C885FC2A26Cull, 0x8880EF183D9F2BF3ull, 0xB2930BDB5CA88C45ull,
-    0x9C2EC8322E1C1553ull, 0xE5B05EAF3220A674ull, 0xA49CC6AE4B861C4Eull, 0x11708E0AEB86EBD7ull,
-    0xC09DE92BBC3902E0ull, 0x929B3C79516BCBC1ull, 0xE006E5BF738F27D1ull, 0x2D9E1EC0EAC8EA38ull,
-    0x0984D8D94BF937C5ull, 0x4959273C220E6747ull, 0xFE1D934207E796FAull, 0x2B9B9298F2F6DD73ull,
-    0x07A1F5A67D6E3A41ull, 0x4407593EE73743D9ull, 0x9F054720EF802E59ull, 0x78D4B711336E6AA6ull,
-    0xADC638AEF3C8B228ull, 0xA4D6D3E86AFB2114ull, 0x9D4808E725531968ull, 0x369804DF3866D0EFull,
-    0xE6DBD9A9D2215024ull, 0x8ED22CA212EE85B2ull, 0x397BB882FCD23EB6ull, 0xEB8F8786D7277531ull,
-    0x9999D4CDAFF543B5ull, 0xF382A61217F192D6ull, 0x49C37260B026ADC1ull, 0x3FF8918CE35C1019ull,
-    0x2E7DF8B76080BD07ull, 0xF5DBAC250B8A28B9ull, 0x853C3727AE9DA4CCull, 0xB2F1F5F3D9E5A26Dull,
-    0x3FCE22012D337847ull, 0x6B5A3E6DB7EEE347ull, 0x171582CD59DDE50Dull, 0xC0C0B3095EE62A8Aull,
-    0x665B25C6F6A203D2ull, 0x3099AED93B6AE69Full, 0x801DF6092BE69C38ull, 0x8066AD0CDFFF43CDull,
-    0x8AF9D44A5F4FDC6Bull, 0xD80219CD97C0D762ull, 0x10C9CEBA14148EBBull, 0x539BD4C3F2F24474ull};
+// Round constants of Tip5 (tip5_params.h).  The MDS first column is inlined
+// in t5_mds below as FP64 literals.
+__device__ __constant__ uint64_t c_t5_rc[T5_ROUNDS * T5_STATE] = {TVMC_T5_ROUND_CONSTANTS};
 
 // Shared-memory S-box table: word w of lane l holds table bytes 4w..4w+3.
 constexpr int T5_SBOX_WORDS = 64 * 32;
@@ -117,8 +97,7 @@ __device__ __forceinline__ uint64_t t5_d_to_u52(double d) {
 // recombined as lo + hi*2^32 with one 128-bit reduction per word.  Moving this
 // work off the integer pipes leaves them to the S-box arithmetic.
 __device__ __forceinline__ void t5_mds(uint64_t s[T5_STATE]) {
-    const double M[T5_STATE] = {61402, 1108, 28750, 33823, 7454, 43244, 53865, 12034,
-                                56951, 27521, 41351, 40901, 12021, 59689, 26798, 17845};
+    const double M[T5_STATE] = {TVMC_T5_MDS_FIRST_COLUMN};
     double dl[T5_STATE], dh[T5_STATE];
 #pragma unroll
     for (int c = 0; c < T5_STATE; c++) {
@@ -171,6 +150,17 @@ __device__ __forceinline__ void t5_permutation(uint64_t s[T5_STATE], const uint3
 #pragma unroll
         for (int i = 0; i < T5_STATE; i++) s[i] = gl_add_pc(s[i], c_t5_rc[rnd * T5_STATE + i]);
     }
+}
+
+// One round (Tip5::round, src/hash/tip5.cpp:114-118) for the off-path
+// single-round and trace entry points; the hashing kernels use t5_permutation.
+__device__ __forceinline__ void t5_round(uint64_t s[T5_STATE], const uint32_t* lane_tbl, int rnd) {
+#pragma unroll
+    for (int i = 0; i < 4; i++) s[i] = t5_split_lookup(s[i], lane_tbl);
+    t5_pow7_layer(s);
+    t5_mds(s);
+#pragma unroll
+    for (int i = 0; i < T5_STATE; i++) s[i] = gl_add_pc(s[i], c_t5_rc[rnd * T5_STATE + i]);
 }
 
 // Tip5::hash_pair / hash_10: rate = left || right, capacity = 1s.

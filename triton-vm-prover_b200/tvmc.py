@@ -26,6 +26,7 @@ DISCARD_LDE = 0x4
 SYNC = 0x8
 PROFILE = 0x10
 FRUGAL = 0x20
+RAND_TRUNCATE = 0x40
 
 _u64p = ctypes.POINTER(ctypes.c_uint64)
 _szp = ctypes.POINTER(ctypes.c_size_t)
@@ -62,6 +63,10 @@ SIGNATURES = {
     "tvmc_ntt_host": (ctypes.c_int, [_u64p, _sz, _sz, ctypes.c_int]),
     "tvmc_lde_batch_gpu": (ctypes.c_int, [_vp, _sz, _sz, _vp, _sz, ctypes.c_uint64, ctypes.c_uint64, _vp]),
     "tvmc_lde_host": (ctypes.c_int, [_u64p, _sz, _sz, _u64p, _sz, ctypes.c_uint64]),
+    "tvmc_lde_randomized_gpu": (ctypes.c_int, [_vp, _sz, _sz, _vp, _sz, _vp, _sz, ctypes.c_uint64,
+                                               ctypes.c_uint64, ctypes.c_uint32, _vp]),
+    "tvmc_lde_randomized_host": (ctypes.c_int, [_u64p, _sz, _sz, _u64p, _sz, _u64p, _sz, ctypes.c_uint64,
+                                                ctypes.c_uint64, ctypes.c_uint32]),
     "tvmc_lde_batch_noalloc_gpu": (ctypes.c_int, [_vp, _sz, _sz, _vp, _sz, ctypes.c_uint64, ctypes.c_uint64,
                                                   _vp]),
     "tvmc_hash_bfield_rows_gpu": (ctypes.c_int, [_vp, _sz, _sz, _vp, _vp]),
@@ -71,11 +76,19 @@ SIGNATURES = {
     "tvmc_hash_pairs_host": (ctypes.c_int, [_u64p, _u64p, _u64p, _sz]),
     "tvmc_tip5_permutation_batch_gpu": (ctypes.c_int, [_vp, _sz, _vp]),
     "tvmc_tip5_permutation_batch_host": (ctypes.c_int, [_u64p, _sz]),
+    "tvmc_tip5_rounds_host": (ctypes.c_int, [_u64p, _sz, ctypes.c_uint32, ctypes.c_uint32, _u64p]),
+    "tvmc_tip5_parameters": (ctypes.c_int, [ctypes.POINTER(ctypes.c_uint8), _u64p, _u64p]),
+    "tvmc_evaluate_on_coset_gpu": (ctypes.c_int, [_vp, _sz, _sz, _vp, _sz, ctypes.c_uint64, _vp]),
+    "tvmc_evaluate_on_coset_host": (ctypes.c_int, [_u64p, _sz, _sz, _u64p, _sz, ctypes.c_uint64]),
+    "tvmc_merkle_root_from_paths_gpu": (ctypes.c_int, [_vp, _vp, _vp, _sz, _sz, _vp, _vp]),
+    "tvmc_merkle_root_from_paths_host": (ctypes.c_int, [_szp, _u64p, _u64p, _sz, _sz, _u64p]),
     "tvmc_merkle_tree_gpu": (ctypes.c_int, [_vp, _vp, _sz, _vp]),
     "tvmc_merkle_root_gpu": (ctypes.c_int, [_vp, _vp, _sz, _vp]),
     "tvmc_merkle_tree_heap_host": (ctypes.c_int, [_u64p, _sz, _u64p]),
     "tvmc_commit": (ctypes.c_int, [_vp, _sz, _sz, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint32, _vp,
                                    ctypes.POINTER(_vp)]),
+    "tvmc_commit_randomized": (ctypes.c_int, [_vp, _sz, _sz, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64,
+                                              _vp, _sz, ctypes.c_uint32, _vp, ctypes.POINTER(_vp)]),
     "tvmc_commitment_root": (ctypes.c_int, [_vp, _u64p]),
     "tvmc_commitment_sync": (ctypes.c_int, [_vp]),
     "tvmc_commitment_shape": (ctypes.c_int, [_vp, _szp, _szp]),
@@ -147,6 +160,59 @@ def ntt(data, inverse: bool = False) -> np.ndarray:
     cols, n = (1, a.size) if a.ndim == 1 else a.shape
     _check(lib().tvmc_ntt_host(_p(a), n, cols, int(inverse)))
     return a
+
+
+def lde_randomized(trace_cm, randomizers, expansion: int = 4, offset: int = 7, trace_offset: int = 1,
+                   truncate: bool = False) -> np.ndarray:
+    """RandomizedLDE::extend_column_with_randomizer on each row of (width, n);
+    randomizers is (width, R).  truncate selects the XFieldElement variants' truncation."""
+    t = _u64(trace_cm)
+    w, n = t.shape
+    r = _u64(randomizers).reshape(w, -1)
+    out = np.empty((w, n * expansion), dtype=np.uint64)
+    _check(lib().tvmc_lde_randomized_host(_p(t), w, n, _p(r) if r.size else None, r.shape[1], _p(out),
+                                          n * expansion, trace_offset, offset, RAND_TRUNCATE if truncate else 0))
+    return out
+
+
+def evaluate_on_coset(coeffs, domain_len: int, offset: int) -> np.ndarray:
+    """NTT::evaluate_on_coset of each row of a (cols, n) array (or a 1-D array)."""
+    a = _u64(coeffs)
+    one = a.ndim == 1
+    a2 = a.reshape(1, -1) if one else a
+    cols, n = a2.shape
+    out = np.empty((cols, domain_len), dtype=np.uint64)
+    _check(lib().tvmc_evaluate_on_coset_host(_p(a2) if a2.size else None, n, cols, _p(out), domain_len, offset))
+    return out[0] if one else out
+
+
+def tip5_rounds(states, first_round: int, num_rounds: int, trace: bool = False):
+    """Tip5 rounds on (count, 16) states; with trace, also (count, num_rounds, 16)."""
+    s = _u64(states).reshape(-1, 16).copy()
+    tr = np.zeros((s.shape[0], num_rounds, 16), dtype=np.uint64) if trace else None
+    _check(lib().tvmc_tip5_rounds_host(_p(s), s.shape[0], first_round, num_rounds,
+                                       _p(tr) if trace and tr.size else None))
+    return (s, tr) if trace else s
+
+
+def tip5_parameters():
+    """(lookup table (256,) u8, MDS first column (16,), round constants (80,))."""
+    lk = np.zeros(256, dtype=np.uint8)
+    mds = np.zeros(16, dtype=np.uint64)
+    rc = np.zeros(80, dtype=np.uint64)
+    _check(lib().tvmc_tip5_parameters(lk.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), _p(mds), _p(rc)))
+    return lk, mds, rc
+
+
+def merkle_roots_from_paths(leaf_idx, leaves, paths) -> np.ndarray:
+    """Root implied by each (index, leaf digest, path (len, 5)) triple."""
+    ix = np.ascontiguousarray(leaf_idx, dtype=np.uintp)
+    lv = _u64(leaves).reshape(-1, 5)
+    pp = _u64(paths).reshape(ix.size, -1, 5)
+    out = np.zeros((ix.size, 5), dtype=np.uint64)
+    _check(lib().tvmc_merkle_root_from_paths_host(ix.ctypes.data_as(_szp), _p(lv), _p(pp) if pp.size else None,
+                                                  ix.size, pp.shape[1], _p(out)))
+    return out
 
 
 def lde(trace_cm, expansion: int = 4, offset: int = 7) -> np.ndarray:
@@ -226,6 +292,12 @@ def lde_gpu(d_trace: int, cols: int, n: int, d_out: int, L: int, offset: int = 7
     _check(lib().tvmc_lde_batch_gpu(d_trace, cols, n, d_out, L, 1, offset, _stream(stream)))
 
 
+def lde_randomized_gpu(d_trace: int, cols: int, n: int, d_rnd: int, R: int, d_out: int, L: int, offset: int = 7,
+                       trace_offset: int = 1, truncate: bool = False, stream=None) -> None:
+    _check(lib().tvmc_lde_randomized_gpu(d_trace, cols, n, d_rnd or None, R, d_out, L, trace_offset, offset,
+                                         RAND_TRUNCATE if truncate else 0, _stream(stream)))
+
+
 def hash_rows_gpu(d_table: int, rows: int, cols: int, d_digests: int, stream=None) -> None:
     _check(lib().tvmc_hash_bfield_rows_gpu(d_table, rows, cols, d_digests, _stream(stream)))
 
@@ -260,8 +332,11 @@ class Commitment:
 
     def __init__(self, trace, width: int | None = None, trace_len: int | None = None, expansion: int = 4,
                  offset: int = 7, row_major: bool = False, device_ptr: bool = False, discard_lde: bool = False,
-                 stream=None, sync: bool = False, profile: bool = False, frugal: bool = False):
-        flags = (PROFILE if profile else 0) | (FRUGAL if frugal else 0)
+                 stream=None, sync: bool = False, profile: bool = False, frugal: bool = False,
+                 randomizers=None, trace_offset: int = 1, truncate: bool = False):
+        """randomizers: host (width, R) array, or with device_ptr=True a device
+        pointer to width*R words given as (pointer, R)."""
+        flags = (PROFILE if profile else 0) | (FRUGAL if frugal else 0) | (RAND_TRUNCATE if truncate else 0)
         if device_ptr:
             flags |= TRACE_DEVICE
             ptr = int(trace)
@@ -281,8 +356,17 @@ class Commitment:
             flags |= DISCARD_LDE
         if sync:
             flags |= SYNC
+        rptr, R = None, 0
+        if randomizers is not None:
+            if device_ptr:
+                rptr, R = int(randomizers[0]), int(randomizers[1])
+            else:
+                r = _u64(randomizers).reshape(width, -1)
+                self._keep_r = r
+                rptr, R = (r.ctypes.data if r.size else None), r.shape[1]
         h = _vp()
-        _check(lib().tvmc_commit(ptr, trace_len, width, expansion, offset, flags, _stream(stream), ctypes.byref(h)))
+        _check(lib().tvmc_commit_randomized(ptr, trace_len, width, expansion, trace_offset, offset, rptr, R, flags,
+                                            _stream(stream), ctypes.byref(h)))
         self.h = h
         self.width = width
         self.trace_len = trace_len
