@@ -16,6 +16,17 @@ measured int32 issue peak; `roofline_lde` = the LDE kernels against HBM;
 sample on this host's cores.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Further workloads (one JSON line each, one GPU):
+    --workload batch     32 tables, heights 2^12..2^18 log-uniform by seed, widths
+                         379 / 264 limbs 50/50, one graph-captured batch launch
+                         (worker streams autotuned) vs committing each alone
+    --workload frugal    2^22 x 379, x4 -> 2^24-row LDE streamed in 10-column
+                         stripes (stripe width autotuned) vs the materialised commit
+    --workload serving   Poisson arrivals of requests with heights 2^10..2^20
+                         log-uniform and widths 379 / 264, 80 openings each, at swept
+                         rates: p50/p99 latency and throughput of the serving loop
+                         vs the plain per-request drop-in
 """
 from __future__ import annotations
 
@@ -373,6 +384,214 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def _seeded_shapes(seed: int, count: int, lo: int, hi: int):
+    rng = np.random.default_rng(seed)
+    logs = rng.integers(lo, hi + 1, count)
+    widths = rng.choice([W_MAIN, W_AUX], count)
+    return [(1 << int(l), int(w)) for l, w in zip(logs, widths)]
+
+
+def _event_ms(torch, stream, fn, reps):
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def run_batch(args):
+    """32 uneven tables committed by one graph launch vs each committed alone."""
+    import torch
+    import tvmc
+    import autotune
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream(dev)
+    shapes = _seeded_shapes(0x7E5EED03, 32, 12, 18)
+    traces = [random_trace(torch, w, n, 3000 + i, dev) for i, (n, w) in enumerate(shapes)]
+    cells = sum(EXPANSION * n * w for n, w in shapes)
+
+    import ctypes
+    cudart = ctypes.CDLL("libcudart.so.12")
+
+    def fill(b):  # device-to-device copies into the batch's own input buffers
+        for i, t in enumerate(traces):
+            cudart.cudaMemcpy(ctypes.c_void_p(b.input_ptr(i)), ctypes.c_void_p(t.data_ptr()),
+                              ctypes.c_size_t(t.numel() * 8), 3)
+        torch.cuda.synchronize()
+
+    tuned = autotune.tune_batch(shapes, fill)
+    with tvmc.Batch(shapes) as b:
+        fill(b)
+        torch.cuda.synchronize()
+        for _ in range(args.warmup):
+            b.run(stream.cuda_stream)
+        launches0 = tvmc.lib().tvmc_launch_count()
+        with ClockSampler(0) as clk:
+            ms = _event_ms(torch, stream, lambda: b.run(stream.cuda_stream), args.steps)
+        launches = (tvmc.lib().tvmc_launch_count() - launches0) // args.steps
+        roots = b.roots()
+
+    def alone():
+        for t, (n, w) in zip(traces, shapes):
+            c = tvmc.Commitment(t.data_ptr(), width=w, trace_len=n, device_ptr=True, stream=stream.cuda_stream,
+                                discard_lde=True)
+            c.free()
+
+    for _ in range(args.warmup):
+        alone()
+    ms_alone = _event_ms(torch, stream, alone, args.steps)
+    match = True
+    for i, (t, (n, w)) in enumerate(zip(traces, shapes)):
+        with tvmc.Commitment(t.data_ptr(), width=w, trace_len=n, device_ptr=True) as c:
+            match = match and bool((c.root() == roots[i]).all())
+    line = {"metric": "committed LDE cells/s", "workload": "batch", "value": cells / (ms / 1e3), "unit": "cells/s",
+            "ms_per_batch": ms, "alone_ms": ms_alone, "speedup_vs_alone": ms_alone / ms,
+            "roots_equal_alone": match, "steps": args.steps, "warmup": args.warmup, "n_gpus": 1,
+            "config": {"tables": len(shapes), "heights": [n for n, _ in shapes], "widths": [w for _, w in shapes],
+                       "expansion": EXPANSION, "cells": cells, "tuning": tuned.get("knobs", {}),
+                       "tuning_s": tuned.get("seconds", {})},
+            "gpu_launches_per_batch": launches, "clocks": clk.summary(), "data": "synthetic uniform field elements"}
+    print(json.dumps(line), flush=True)
+
+
+def run_frugal(args):
+    """2^22 x 379 streamed in stripes (the full LDE never exists) vs materialised."""
+    import torch
+    import tvmc
+    import autotune
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream(dev)
+    log_n = args.log_n if args.log_n != LOG_N else 22
+    n, w = 1 << log_n, W_MAIN
+    trace = random_trace(torch, w, n, 4000, dev)
+    cells = EXPANSION * n * w
+    tuned = autotune.tune_frugal(trace.data_ptr(), n, w)
+
+    def commit(frugal):
+        c = tvmc.Commitment(trace.data_ptr(), width=w, trace_len=n, device_ptr=True, stream=stream.cuda_stream,
+                            frugal=frugal, discard_lde=True)
+        c.free()
+
+    for _ in range(args.warmup):
+        commit(True)
+    free0 = torch.cuda.mem_get_info(dev)[0]
+    with ClockSampler(0) as clk:
+        ms = _event_ms(torch, stream, lambda: commit(True), args.steps)
+    for _ in range(1):
+        commit(False)
+    ms_mat = _event_ms(torch, stream, lambda: commit(False), max(1, args.steps // 2))
+    with tvmc.Commitment(trace.data_ptr(), width=w, trace_len=n, device_ptr=True, frugal=True) as a, \
+            tvmc.Commitment(trace.data_ptr(), width=w, trace_len=n, device_ptr=True, discard_lde=True) as b:
+        same = bool((a.root() == b.root()).all())
+    line = {"metric": "committed LDE cells/s", "workload": "frugal", "value": cells / (ms / 1e3), "unit": "cells/s",
+            "ms_per_commit": ms, "materialised_ms": ms_mat, "root_equals_materialised": same,
+            "lde_bytes_if_materialised": cells * 8, "steps": args.steps, "warmup": args.warmup, "n_gpus": 1,
+            "config": {"trace_len": n, "width": w, "expansion": EXPANSION, "tuning": tuned.get("knobs", {}),
+                       "tuning_s": tuned.get("seconds", {}), "free_bytes_before_timing": free0},
+            "clocks": clk.summary(), "data": "synthetic uniform field elements"}
+    print(json.dumps(line), flush=True)
+
+
+def run_serving(args):
+    """Poisson arrivals, mixed sizes, 80 openings per request: serving loop vs
+    the plain per-request drop-in (one commit at a time, in arrival order)."""
+    import threading
+    import torch
+    import tvmc
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    rng = np.random.default_rng(0x7E5EED05)
+    M = args.requests
+    shapes = _seeded_shapes(0x7E5EED05, M, 10, args.serve_max_log_n)
+    host = {}
+    for (n, w) in sorted(set(shapes)):  # one pinned host table per shape class
+        d = random_trace(torch, w, n, 5000 + n + w, dev)
+        h = torch.empty((w, n), dtype=torch.int64, pin_memory=True)
+        h.copy_(d)
+        host[(n, w)] = h
+        del d
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    reqs = [host[sh].numpy().view(np.uint64) for sh in shapes]
+    opens = [rng.integers(0, EXPANSION * n, 80) for n, _ in shapes]
+    cells = [EXPANSION * n * w for n, w in shapes]
+    st = torch.cuda.Stream(dev)
+
+    def plain(arr_ns):
+        lat = []
+        t0 = time.monotonic_ns() + 20_000_000
+        for i, t in enumerate(reqs):
+            target = t0 + arr_ns[i]
+            while time.monotonic_ns() < target:
+                time.sleep(max(0.0, (target - time.monotonic_ns()) / 1e9 - 0.0005))
+            c = tvmc.Commitment(t, stream=st.cuda_stream, discard_lde=True)
+            c.root()
+            lat.append(time.monotonic_ns() - target)
+            c.auth_paths(opens[i])
+            c.free()
+        return lat, (time.monotonic_ns() - t0 - arr_ns[0]) / 1e9
+
+    def served(arr_ns):
+        lat = [0] * M
+        ids = [None] * M
+        ready = [threading.Event() for _ in range(M)]
+        t0 = time.monotonic_ns() + 20_000_000
+        with tvmc.Server(streams=args.serve_streams) as srv:
+            def waiter():
+                for i in range(M):
+                    ready[i].wait()
+                    srv.wait(ids[i])
+                    srv.open(ids[i], opens[i])
+                    lat[i] = srv.times(ids[i])[2] - (t0 + arr_ns[i])
+                    srv.release(ids[i])
+            th = threading.Thread(target=waiter)
+            th.start()
+            for i, t in enumerate(reqs):
+                target = t0 + arr_ns[i]
+                while time.monotonic_ns() < target:
+                    time.sleep(max(0.0, (target - time.monotonic_ns()) / 1e9 - 0.0005))
+                ids[i] = srv.submit(t)
+                ready[i].set()
+            th.join()
+            stats = srv.stats()
+        return lat, (time.monotonic_ns() - t0 - arr_ns[0]) / 1e9, stats
+
+    def summ(lat, span):
+        ms = np.array(lat) / 1e6
+        return {"p50_ms": float(np.percentile(ms, 50)), "p99_ms": float(np.percentile(ms, 99)),
+                "mean_ms": float(ms.mean()), "throughput_rps": M / span, "cells_per_s": sum(cells) / span}
+
+    zero = [0] * M
+    plain(zero)  # warm-up: twiddle tables, pool, pinned paths
+    served(zero)
+    lat0, span0 = plain(zero)  # back-to-back: the plain path's service time
+    service_s = span0 / M
+    rates = []
+    for rho in args.serve_loads:
+        lam = rho / service_s
+        gaps = np.random.default_rng(int(rho * 1000)).exponential(1.0 / lam, M)
+        arr = (np.cumsum(gaps) - gaps[0]) * 1e9
+        arr_ns = [int(x) for x in arr]
+        pl, pspan = plain(arr_ns)
+        sv, sspan, stats = served(arr_ns)
+        rates.append({"load_vs_plain_capacity": rho, "rate_rps": lam, "plain": summ(pl, pspan),
+                      "server": summ(sv, sspan), "server_peak_bytes": stats["bytes_peak"],
+                      "server_budget_bytes": stats["budget"]})
+    line = {"metric": "serving latency p50/p99 and throughput", "workload": "serving", "requests": M,
+            "plain_service_ms_mean": 1e3 * service_s,
+            "config": {"heights": f"2^10..2^{args.serve_max_log_n} log-uniform", "widths": [W_MAIN, W_AUX],
+                       "expansion": EXPANSION, "openings_per_request": 80, "server_streams": args.serve_streams,
+                       "host_buffers": "pinned, one per (height, width) class",
+                       "latency": "arrival -> root committed (server: completion callback time)"},
+            "rates": rates, "n_gpus": 1, "data": "synthetic uniform field elements"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -384,10 +603,22 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--width-main", type=int, default=W_MAIN, help="main-table columns (profiling sizes)")
     ap.add_argument("--width-aux", type=int, default=W_AUX, help="aux-table base limbs (profiling sizes)")
+    ap.add_argument("--workload", choices=["commit", "batch", "frugal", "serving"], default="commit")
+    ap.add_argument("--requests", type=int, default=48, help="serving: requests per rate")
+    ap.add_argument("--serve-streams", type=int, default=4)
+    ap.add_argument("--serve-max-log-n", type=int, default=20)
+    ap.add_argument("--serve-loads", type=float, nargs="+", default=[0.5, 0.9, 1.5, 3.0],
+                    help="serving: offered load as a multiple of the plain path's capacity")
     args = ap.parse_args()
     globals()["W_MAIN"], globals()["W_AUX"] = args.width_main, args.width_aux
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "batch":
+        run_batch(args)
+    elif args.workload == "frugal":
+        run_frugal(args)
+    elif args.workload == "serving":
+        run_serving(args)
     else:
         run_ours(args)
 

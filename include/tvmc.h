@@ -288,6 +288,58 @@ int tvmc_batch_run(tvmc_batch* b, void* stream);
 int tvmc_batch_commitment(tvmc_batch* b, size_t i, tvmc_commitment** c);
 int tvmc_batch_free(tvmc_batch* b);
 
+/* ---- commitment serving (no reference counterpart: the reference commits one
+ *      table at a time in src/stark.cpp:1163-1196) ----
+ *
+ * A server runs a request loop on the current device: submitted tables queue
+ * in arrival order; the head is admitted as soon as its device footprint
+ * (tree, LDE, LDE scratch, upload staging) fits the HBM budget beside the
+ * running requests and the trees still held, and is issued at once on the
+ * least-loaded of its worker streams (small tables on high-priority streams),
+ * so requests of mixed sizes run concurrently as they arrive.  Each request's
+ * Merkle tree stays on the device for openings until tvmc_server_release;
+ * with TVMC_SERVER_KEEP_LDE its LDE stays too (rows can be opened).  Results
+ * are bit-identical to tvmc_commit of the same table alone.  The trace buffer
+ * must stay valid until tvmc_server_wait has returned for the request.  All
+ * functions are thread-safe. */
+typedef struct tvmc_server tvmc_server;
+
+#define TVMC_SERVER_KEEP_LDE 0x1u
+
+typedef struct tvmc_server_config {
+    size_t hbm_budget_bytes; /* 0: 90% of the device memory free at creation */
+    uint32_t num_streams;    /* worker streams, 0: 4 (at most 64) */
+    uint32_t flags;          /* TVMC_SERVER_KEEP_LDE */
+} tvmc_server_config;
+
+typedef struct tvmc_server_stats {
+    uint64_t submitted, completed, failed, released, queued, running;
+    size_t bytes_in_use, bytes_peak, budget; /* admitted footprint bytes */
+} tvmc_server_stats;
+
+int tvmc_server_create(const tvmc_server_config* cfg, tvmc_server** out);
+/* Queue one table (the arguments of tvmc_commit; flags may hold only
+ * TVMC_TRACE_DEVICE, TVMC_TRACE_ROW_MAJOR and TVMC_FRUGAL). */
+int tvmc_server_submit(tvmc_server* s, const uint64_t* trace, size_t trace_len, size_t width, uint32_t expansion,
+                       uint64_t offset, uint32_t flags, uint64_t* request_id);
+/* Wait until the request is committed (timeout_ms < 0: no limit; expiry returns
+ * TVMC_ERR_TIMEOUT) and copy its root; a request whose footprint exceeds the
+ * whole budget fails with TVMC_ERR_NOMEM. */
+int tvmc_server_wait(tvmc_server* s, uint64_t request_id, int64_t timeout_ms, uint64_t* root);
+/* Openings of a committed request from its device-resident tree: auth paths
+ * (count x height x 5 words, as tvmc_commitment_auth_paths) and, when the
+ * server keeps LDEs and rows is non-null, the opened rows (count x width). */
+int tvmc_server_open(tvmc_server* s, uint64_t request_id, const size_t* leaf_idx, size_t count, uint64_t* paths,
+                     uint64_t* rows);
+/* Submission, dispatch and completion times (CLOCK_MONOTONIC nanoseconds). */
+int tvmc_server_times(tvmc_server* s, uint64_t request_id, uint64_t* submit_ns, uint64_t* start_ns,
+                      uint64_t* done_ns);
+/* Free a finished request's tree (and LDE) and return its bytes to the budget. */
+int tvmc_server_release(tvmc_server* s, uint64_t request_id);
+int tvmc_server_get_stats(tvmc_server* s, tvmc_server_stats* out);
+/* Stops dispatching, waits for running requests and frees everything. */
+int tvmc_server_destroy(tvmc_server* s);
+
 /* For a TVMC_PROFILE commitment: device milliseconds of [upload (or transpose),
  * LDE, row hash + Merkle tree]; with a pipelined host upload the upload is
  * counted inside the LDE phase. */

@@ -1,0 +1,117 @@
+"""The commitment serving loop (tvmc_server_*): every request's root, tree
+openings and rows are bit-identical to committing that table alone, whatever
+else is in flight; admission respects the HBM budget; errors and timeouts are
+reported per request."""
+import threading
+
+import numpy as np
+import pytest
+
+from conftest import rand_u64
+
+pytestmark = pytest.mark.gpu
+
+
+def _mix(seed, count, logs=(4, 6, 8, 10, 12, 14), widths=(379, 264, 23)):
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = 1 << int(rng.choice(logs))
+        w = int(rng.choice(widths))
+        out.append(rand_u64(seed * 1000 + i, (w, n)))
+    return out
+
+
+@pytest.mark.parametrize("streams,budget", [(4, 0), (1, 0), (8, 600 << 20)])
+def test_server_results_equal_alone(tv, streams, budget):
+    """A mix of sizes submitted at once (a tight budget forces queueing):
+    roots and 80 openings per request equal each table committed alone."""
+    tables = _mix(7 + streams, 14)
+    rng = np.random.default_rng(3)
+    with tv.Server(hbm_budget_bytes=budget, streams=streams) as srv:
+        ids = [srv.submit(t) for t in tables]
+        for rid, t in zip(ids, tables):
+            root = srv.wait(rid)
+            L = 4 * t.shape[1]
+            idx = rng.integers(0, L, 80)
+            with tv.Commitment(t) as alone:
+                assert (root == alone.root()).all()
+                assert (srv.open(rid, idx) == alone.auth_paths(idx)).all()
+            srv.release(rid)
+        st = srv.stats()
+        assert st["completed"] == len(tables) and st["failed"] == 0 and st["bytes_in_use"] == 0
+        if budget:
+            assert st["bytes_peak"] <= budget
+
+
+def test_server_keep_lde_rows_and_layouts(tv):
+    t = rand_u64(11, (37, 1 << 9))
+    with tv.Server(keep_lde=True) as srv:
+        a = srv.submit(t)
+        b = srv.submit(np.ascontiguousarray(t.T), row_major=True)
+        c = srv.submit(t, frugal=True)
+        with tv.Commitment(t) as alone:
+            for rid in (a, b, c):
+                assert (srv.wait(rid) == alone.root()).all()
+            idx = [0, 5, 2047, 1000]
+            paths, rows = srv.open(a, idx, rows=True)
+            assert (paths == alone.auth_paths(idx)).all()
+            assert (rows == alone.read_rows(idx)).all()
+        with pytest.raises(tv.InvalidArgument):  # frugal requests keep no LDE
+            srv.open(c, idx, rows=True)
+        with pytest.raises(tv.OutOfRange):
+            srv.open(a, [4 * 512])
+
+
+def test_server_concurrent_submitters(tv):
+    """Four host threads submitting and waiting at once."""
+    tables = _mix(21, 16, logs=(6, 8, 10))
+    results = {}
+    with tv.Server(streams=4) as srv:
+        def worker(k):
+            for i in range(k, len(tables), 4):
+                rid = srv.submit(tables[i])
+                results[i] = srv.wait(rid)
+                srv.release(rid)
+        th = [threading.Thread(target=worker, args=(k,)) for k in range(4)]
+        for x in th:
+            x.start()
+        for x in th:
+            x.join()
+    for i, t in enumerate(tables):
+        with tv.Commitment(t) as alone:
+            assert (results[i] == alone.root()).all()
+
+
+def test_server_budget_and_errors(tv):
+    big = rand_u64(5, (64, 1 << 12))
+    small = rand_u64(6, (8, 1 << 6))
+    with tv.Server(hbm_budget_bytes=1 << 20) as srv:  # 1 MiB: the big table cannot fit
+        rb = srv.submit(big)
+        rs = srv.submit(small)
+        with pytest.raises(tv.OutOfMemory):
+            srv.wait(rb)
+        with tv.Commitment(small) as alone:
+            assert (srv.wait(rs) == alone.root()).all()
+        srv.release(rb)  # failed requests can be released
+        srv.release(rs)
+        with pytest.raises(tv.InvalidArgument):
+            srv.release(rs)
+        with pytest.raises(tv.InvalidArgument):
+            srv.submit(rand_u64(1, (3, 12)))  # not a power of two
+        assert srv.stats()["failed"] == 1
+
+
+def test_server_wait_timeout_and_times(tv):
+    t = rand_u64(9, (379, 1 << 14))
+    with tv.Server() as srv:
+        rid = srv.submit(t)
+        try:
+            srv.wait(rid, timeout_ms=0)
+        except tv.Timeout:
+            pass  # still running: the bounded wait returned without blocking
+        srv.wait(rid)
+        sub, start, done = srv.times(rid)
+        assert 0 < sub <= start <= done
+        with pytest.raises(tv.InvalidArgument):
+            srv.wait(rid + 1000)

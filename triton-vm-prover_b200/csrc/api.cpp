@@ -399,6 +399,30 @@ int host_buf(size_t words, HostBuf* hb) {
     return TVMC_OK;
 }
 
+// Per-thread, per-device non-blocking stream for the small synchronous reads
+// (openings): they neither queue behind other streams' commits nor, having no
+// cudaFree, stall the device.
+struct AccStreams {
+    std::map<int, cudaStream_t> s;
+    ~AccStreams() {
+        for (auto& kv : s) cudaStreamDestroy(kv.second);
+    }
+};
+thread_local AccStreams t_acc;
+
+int acc_stream(cudaStream_t* out) {
+    int dev;
+    CK(cudaGetDevice(&dev));
+    auto it = t_acc.s.find(dev);
+    if (it == t_acc.s.end()) {
+        cudaStream_t st;
+        CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        it = t_acc.s.emplace(dev, st).first;
+    }
+    *out = it->second;
+    return TVMC_OK;
+}
+
 // TVMC_FRUGAL commit: the LDE is produced stripe by stripe (10-column aligned)
 // and each stripe is absorbed at once into the per-row sponge capacity state,
 // so only one stripe of LDE (plus 48 bytes of state per row) is ever resident.
@@ -533,6 +557,40 @@ struct tvmc_batch {
     cudaGraphExec_t exec = nullptr;
     unsigned long long kernels_per_run = 0;
 };
+
+namespace {
+// Index list -> device, a gather kernel, result -> host, all on the calling
+// thread's accessor stream after the commitment's completion event; per_item
+// output words per index.
+template <typename Gather>
+int gather_sync(const tvmc_commitment* c, const void* idx, size_t count, size_t per_item, uint64_t* out,
+                Gather gather) {
+    static_assert(sizeof(size_t) == 8, "64-bit indices");
+    cudaStream_t st;
+    int rc = acc_stream(&st);
+    if (rc) return rc;
+    HostBuf hb;
+    if ((rc = host_buf(count * (1 + per_item), &hb))) return rc;
+    uint64_t *di = hb.p, *dout = hb.p + count;
+    CK(cudaStreamWaitEvent(st, c->done, 0));
+    CK(cudaMemcpyAsync(di, idx, count * 8, cudaMemcpyHostToDevice, st));
+    CK(gather(di, dout, st));
+    CK(cudaMemcpyAsync(out, dout, count * per_item * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return TVMC_OK;
+}
+
+// Device words -> host after the commitment's completion, on the accessor stream.
+int read_sync(const tvmc_commitment* c, const uint64_t* src, size_t words, uint64_t* out) {
+    cudaStream_t st;
+    int rc = acc_stream(&st);
+    if (rc) return rc;
+    CK(cudaStreamWaitEvent(st, c->done, 0));
+    CK(cudaMemcpyAsync(out, src, words * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return TVMC_OK;
+}
+}  // namespace
 
 extern "C" {
 
@@ -1008,9 +1066,7 @@ int tvmc_commitment_sync(tvmc_commitment* c) {
 
 int tvmc_commitment_root(tvmc_commitment* c, uint64_t* root) {
     if (!c || !root) return fail(TVMC_ERR_INVALID, "null argument");
-    CK(cudaEventSynchronize(c->done));
-    CK(cudaMemcpy(root, c->d_nodes + 5, 40, cudaMemcpyDeviceToHost));
-    return TVMC_OK;
+    return read_sync(c, c->d_nodes + 5, 5, root);
 }
 
 int tvmc_commitment_shape(const tvmc_commitment* c, size_t* lde_len, size_t* width) {
@@ -1039,15 +1095,9 @@ int tvmc_commitment_auth_paths(tvmc_commitment* c, const size_t* leaf_idx, size_
         if (leaf_idx[q] >= c->L) return fail(TVMC_ERR_RANGE, "Leaf index %zu out of range", leaf_idx[q]);
     int h = log2u(c->L);
     if (h == 0) return TVMC_OK;
-    std::vector<uint64_t> idx(leaf_idx, leaf_idx + count);
-    DBuf di, dout;
-    CK(di.alloc(count));
-    CK(dout.alloc(count * h * 5));
-    CK(cudaEventSynchronize(c->done));
-    CK(cudaMemcpy(di.p, idx.data(), count * 8, cudaMemcpyHostToDevice));
-    CK(launch_gather_auth_paths(c->d_nodes, c->L, LAYOUT_HEAP, di.p, count, dout.p, nullptr));
-    CK(cudaMemcpy(out, dout.p, count * h * 40, cudaMemcpyDeviceToHost));
-    return TVMC_OK;
+    return gather_sync(c, leaf_idx, count, (size_t)h * 5, out, [&](const uint64_t* di, uint64_t* dout, cudaStream_t st) {
+        return launch_gather_auth_paths(c->d_nodes, c->L, LAYOUT_HEAP, di, count, dout, st);
+    });
 }
 
 int tvmc_auth_structure_indices(size_t num_leaves, const size_t* leaf_idx, size_t count, uint64_t* out,
@@ -1071,14 +1121,9 @@ int tvmc_commitment_auth_structure(tvmc_commitment* c, const size_t* leaf_idx, s
     if (num_digests) *num_digests = res.size();
     size_t m = std::min(res.size(), max_digests);
     if (m == 0) return TVMC_OK;
-    DBuf di, dout;
-    CK(di.alloc(m));
-    CK(dout.alloc(5 * m));
-    CK(cudaEventSynchronize(c->done));
-    CK(cudaMemcpy(di.p, res.data(), m * 8, cudaMemcpyHostToDevice));
-    CK(launch_gather_nodes(c->d_nodes, n, LAYOUT_HEAP, di.p, m, dout.p, nullptr));
-    CK(cudaMemcpy(out, dout.p, m * 40, cudaMemcpyDeviceToHost));
-    return TVMC_OK;
+    return gather_sync(c, res.data(), m, 5, out, [&](const uint64_t* di, uint64_t* dout, cudaStream_t st) {
+        return launch_gather_nodes(c->d_nodes, n, LAYOUT_HEAP, di, m, dout, st);
+    });
 }
 
 int tvmc_commitment_read_rows(tvmc_commitment* c, const size_t* rows, size_t count, uint64_t* out) {
@@ -1087,15 +1132,9 @@ int tvmc_commitment_read_rows(tvmc_commitment* c, const size_t* rows, size_t cou
     for (size_t q = 0; q < count; q++)
         if (rows[q] >= c->L) return fail(TVMC_ERR_RANGE, "Row index %zu out of range", rows[q]);
     if (count == 0 || c->width == 0) return TVMC_OK;
-    std::vector<uint64_t> idx(rows, rows + count);
-    DBuf di, dout;
-    CK(di.alloc(count));
-    CK(dout.alloc(count * c->width));
-    CK(cudaEventSynchronize(c->done));
-    CK(cudaMemcpy(di.p, idx.data(), count * 8, cudaMemcpyHostToDevice));
-    CK(launch_gather_rows(c->d_lde, c->L, (uint32_t)c->width, di.p, count, dout.p, nullptr));
-    CK(cudaMemcpy(out, dout.p, count * c->width * 8, cudaMemcpyDeviceToHost));
-    return TVMC_OK;
+    return gather_sync(c, rows, count, c->width, out, [&](const uint64_t* di, uint64_t* dout, cudaStream_t st) {
+        return launch_gather_rows(c->d_lde, c->L, (uint32_t)c->width, di, count, dout, st);
+    });
 }
 
 int tvmc_commitment_read_columns(tvmc_commitment* c, size_t col0, size_t ncols, uint64_t* out) {
@@ -1128,16 +1167,12 @@ int tvmc_commitment_read_lde(tvmc_commitment* c, uint64_t* out, int row_major) {
 
 int tvmc_commitment_read_leaves(tvmc_commitment* c, uint64_t* out) {
     if (!c) return fail(TVMC_ERR_INVALID, "null handle");
-    CK(cudaEventSynchronize(c->done));
-    CK(cudaMemcpy(out, c->d_nodes + 5 * c->L, c->L * 40, cudaMemcpyDeviceToHost));
-    return TVMC_OK;
+    return read_sync(c, c->d_nodes + 5 * c->L, c->L * 5, out);
 }
 
 int tvmc_commitment_read_nodes(tvmc_commitment* c, uint64_t* out) {
     if (!c) return fail(TVMC_ERR_INVALID, "null handle");
-    CK(cudaEventSynchronize(c->done));
-    CK(cudaMemcpy(out, c->d_nodes, 2 * c->L * 40, cudaMemcpyDeviceToHost));
-    return TVMC_OK;
+    return read_sync(c, c->d_nodes, c->L * 10, out);
 }
 
 int tvmc_commitment_free(tvmc_commitment* c) {

@@ -1,0 +1,359 @@
+// Commitment serving runtime (host C++; the GPU work is tvmc_commit's).
+//
+// A server owns worker streams on one device and a dispatcher thread.
+// Submitted requests queue in arrival order; the dispatcher admits the head of
+// the queue as soon as its device footprint fits the HBM budget next to what
+// running requests and resident trees already hold, and issues it at once on
+// the least-loaded worker stream (small tables on high-priority streams), so
+// requests of mixed sizes run concurrently as they arrive.  A host callback
+// on the stream marks each request done, records its completion time and
+// returns its transient memory to the budget; its Merkle tree (and, with
+// TVMC_SERVER_KEEP_LDE, its LDE) stays on the device for openings until the
+// caller releases it.  The reference has no counterpart: its prover commits
+// one table at a time (src/stark.cpp:1163-1196).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "internal.cuh"
+#include "tvmc.h"
+
+namespace {
+
+uint64_t now_ns() {
+    return (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
+               std::chrono::steady_clock::now().time_since_epoch())
+        .count();
+}
+
+enum class State { Queued, Running, Done, Failed };
+
+struct Request {
+    uint64_t id = 0;
+    const uint64_t* trace = nullptr;
+    size_t n = 0, width = 0;
+    uint32_t expansion = 4, flags = 0;
+    uint64_t offset = 7;
+    size_t resident = 0, transient = 0;  // budget bytes held until release / until done
+    int stream = -1;
+    State state = State::Queued;
+    int status = TVMC_OK;
+    std::string error;
+    tvmc_commitment* c = nullptr;
+    uint64_t t_submit = 0, t_start = 0, t_done = 0;
+};
+
+// Device bytes a request holds: the tree (and a kept LDE) until release; the
+// LDE, LDE scratch, upload staging and frugal state until it completes.
+void footprint(Request* r, bool keep_lde, size_t scratch_budget) {
+    const size_t N = r->n, L = N * r->expansion, W = r->width, NW = N * W * 8;
+    const bool frugal = r->flags & TVMC_FRUGAL, dev = r->flags & TVMC_TRACE_DEVICE,
+               rm = r->flags & TVMC_TRACE_ROW_MAJOR;
+    const size_t tree = 2 * L * 40;
+    const size_t lde = frugal ? std::min<size_t>(L * W * 8, size_t(2) << 30) : L * W * 8;
+    const size_t scratch = N > 2048 ? std::min(scratch_budget, N * (1 + r->expansion) * 8 * std::max<size_t>(W, 1)) : 0;
+    size_t upload = 0;
+    if (frugal) upload = (dev ? 0 : NW) + (rm ? NW : 0) + 6 * L * 8;
+    else if (!dev && !rm) upload = 2 * std::min<size_t>(NW, size_t(256) << 20);
+    else upload = (dev ? 0 : NW) + (rm ? NW : 0);
+    r->resident = tree + (keep_lde && !frugal ? lde : 0);
+    r->transient = (keep_lde && !frugal ? 0 : lde) + scratch + upload;
+}
+
+}  // namespace
+
+struct tvmc_server {
+    int device = 0;
+    size_t budget = 0;
+    bool keep_lde = false;
+    size_t scratch_budget = size_t(2) << 30;
+    std::vector<cudaStream_t> streams;
+    std::vector<int> inflight;  // per stream
+    std::mutex mu;
+    std::condition_variable cv;  // queue changes, completions, releases
+    std::deque<Request*> queue;
+    std::unordered_map<uint64_t, std::unique_ptr<Request>> reqs;
+    size_t used = 0, peak = 0;
+    uint64_t next_id = 1, submitted = 0, completed = 0, failed = 0, released = 0;
+    int running = 0;
+    bool stop = false;
+    std::thread dispatcher;
+};
+
+namespace {
+
+struct DoneCtx {
+    tvmc_server* s;
+    Request* r;
+};
+
+void CUDART_CB on_done(void* p) {
+    std::unique_ptr<DoneCtx> ctx(static_cast<DoneCtx*>(p));
+    tvmc_server* s = ctx->s;
+    std::lock_guard<std::mutex> lk(s->mu);
+    Request* r = ctx->r;
+    r->state = State::Done;
+    r->t_done = now_ns();
+    s->used -= r->transient;
+    s->inflight[r->stream]--;
+    s->running--;
+    s->completed++;
+    s->cv.notify_all();
+}
+
+void fail_request(tvmc_server* s, Request* r, int status, const std::string& msg) {
+    r->state = State::Failed;
+    r->status = status;
+    r->error = msg;
+    r->t_done = now_ns();
+    s->failed++;
+    s->cv.notify_all();
+}
+
+void dispatch_loop(tvmc_server* s) {
+    cudaSetDevice(s->device);
+    std::unique_lock<std::mutex> lk(s->mu);
+    while (true) {
+        s->cv.wait(lk, [&] {
+            if (s->stop) return true;
+            if (s->queue.empty()) return false;
+            Request* r = s->queue.front();
+            return r->resident + r->transient > s->budget || s->used + r->resident + r->transient <= s->budget;
+        });
+        if (s->stop) return;
+        Request* r = s->queue.front();
+        s->queue.pop_front();
+        const size_t need = r->resident + r->transient;
+        if (need > s->budget) {
+            fail_request(s, r, TVMC_ERR_NOMEM, "request footprint exceeds the server's HBM budget");
+            continue;
+        }
+        s->used += need;
+        s->peak = std::max(s->peak, s->used);
+        // small tables to the high-priority half of the streams
+        const bool small = r->n * r->expansion * std::max<size_t>(r->width, 1) <= (size_t(1) << 22);
+        const int half = (int)s->streams.size() / 2;
+        int lo = small ? 0 : half, hi = small ? half : (int)s->streams.size();
+        if (lo == hi) lo = 0, hi = (int)s->streams.size();
+        int best = lo;
+        for (int i = lo; i < hi; i++)
+            if (s->inflight[i] < s->inflight[best]) best = i;
+        r->stream = best;
+        s->inflight[best]++;
+        s->running++;
+        r->state = State::Running;
+        r->t_start = now_ns();
+        const uint32_t flags = (r->flags & (TVMC_TRACE_DEVICE | TVMC_TRACE_ROW_MAJOR | TVMC_FRUGAL)) |
+                               (s->keep_lde ? 0u : (uint32_t)TVMC_DISCARD_LDE);
+        cudaStream_t st = s->streams[best];
+        lk.unlock();
+        tvmc_commitment* c = nullptr;
+        const int rc = tvmc_commit(r->trace, r->n, r->width, r->expansion, r->offset, flags, st, &c);
+        const std::string err = rc ? tvmc_last_error() : "";
+        lk.lock();
+        if (rc) {
+            s->used -= need;
+            s->inflight[best]--;
+            s->running--;
+            fail_request(s, r, rc, err);
+            continue;
+        }
+        r->c = c;  // set before the completion callback can run
+        lk.unlock();
+        auto* ctx = new DoneCtx{s, r};
+        const cudaError_t e = cudaLaunchHostFunc(st, on_done, ctx);
+        lk.lock();
+        if (e != cudaSuccess) {
+            delete ctx;
+            r->c = nullptr;
+            s->used -= need;
+            s->inflight[best]--;
+            s->running--;
+            fail_request(s, r, TVMC_ERR_CUDA, cudaGetErrorString(e));
+            lk.unlock();
+            tvmc_commitment_free(c);
+            lk.lock();
+            continue;
+        }
+        // the resident part stays charged until release; on_done returns the transient part
+    }
+}
+
+Request* find(tvmc_server* s, uint64_t id) {
+    auto it = s->reqs.find(id);
+    return it == s->reqs.end() ? nullptr : it->second.get();
+}
+
+}  // namespace
+
+extern "C" {
+
+int tvmc_server_create(const tvmc_server_config* cfg, tvmc_server** out) {
+    if (!out) return tvmc::set_error(TVMC_ERR_INVALID, "null output handle");
+    *out = nullptr;
+    tvmc_server_config c{};
+    if (cfg) c = *cfg;
+    if (c.flags & ~(uint32_t)TVMC_SERVER_KEEP_LDE) return tvmc::set_error(TVMC_ERR_INVALID, "unknown server flags");
+    auto s = std::make_unique<tvmc_server>();
+    if (cudaGetDevice(&s->device) != cudaSuccess) return tvmc::set_error(TVMC_ERR_CUDA, "no CUDA device");
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return tvmc::set_error(TVMC_ERR_CUDA, "cudaMemGetInfo");
+    s->budget = c.hbm_budget_bytes ? c.hbm_budget_bytes : free_b / 10 * 9;
+    s->keep_lde = c.flags & TVMC_SERVER_KEEP_LDE;
+    long long sb = 0;
+    if (tvmc_get_tuning("lde_scratch_bytes", &sb) == TVMC_OK && sb > 0) s->scratch_budget = (size_t)sb;
+    const int ns = c.num_streams ? (int)std::min<uint32_t>(c.num_streams, 64) : 4;
+    int lo_prio = 0, hi_prio = 0;
+    cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio);
+    for (int i = 0; i < ns; i++) {
+        cudaStream_t st;
+        const int prio = (ns > 1 && i < ns / 2) ? hi_prio : lo_prio;
+        if (cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, prio) != cudaSuccess) {
+            for (auto x : s->streams) cudaStreamDestroy(x);
+            return tvmc::set_error(TVMC_ERR_CUDA, "cannot create worker streams");
+        }
+        s->streams.push_back(st);
+    }
+    s->inflight.assign(ns, 0);
+    tvmc_server* raw = s.release();
+    raw->dispatcher = std::thread(dispatch_loop, raw);
+    *out = raw;
+    return TVMC_OK;
+}
+
+int tvmc_server_submit(tvmc_server* s, const uint64_t* trace, size_t trace_len, size_t width, uint32_t expansion,
+                       uint64_t offset, uint32_t flags, uint64_t* id) {
+    if (!s || !id) return tvmc::set_error(TVMC_ERR_INVALID, "null argument");
+    if (flags & ~(uint32_t)(TVMC_TRACE_DEVICE | TVMC_TRACE_ROW_MAJOR | TVMC_FRUGAL))
+        return tvmc::set_error(TVMC_ERR_INVALID, "server requests take only trace-layout and frugal flags");
+    if (!trace_len || (trace_len & (trace_len - 1)) || trace_len > (size_t(1) << TVMC_MAX_LOG_LDE_TRACE))
+        return tvmc::set_error(TVMC_ERR_INVALID, "trace length is not a supported power of 2");
+    if (!expansion || (expansion & (expansion - 1)) || expansion > 16)
+        return tvmc::set_error(TVMC_ERR_INVALID, "expansion factor is not a power of 2 <= 16");
+    if (width && !trace) return tvmc::set_error(TVMC_ERR_INVALID, "null trace");
+    auto r = std::make_unique<Request>();
+    r->trace = trace;
+    r->n = trace_len;
+    r->width = width;
+    r->expansion = expansion;
+    r->offset = offset;
+    r->flags = flags;
+    r->t_submit = now_ns();
+    std::lock_guard<std::mutex> lk(s->mu);
+    footprint(r.get(), s->keep_lde, s->scratch_budget);
+    r->id = s->next_id++;
+    *id = r->id;
+    s->queue.push_back(r.get());
+    s->reqs.emplace(r->id, std::move(r));
+    s->submitted++;
+    s->cv.notify_all();
+    return TVMC_OK;
+}
+
+int tvmc_server_wait(tvmc_server* s, uint64_t id, int64_t timeout_ms, uint64_t* root) {
+    if (!s) return tvmc::set_error(TVMC_ERR_INVALID, "null server");
+    std::unique_lock<std::mutex> lk(s->mu);
+    Request* r = find(s, id);
+    if (!r) return tvmc::set_error(TVMC_ERR_INVALID, "unknown request id");
+    auto ready = [&] { return r->state == State::Done || r->state == State::Failed; };
+    if (timeout_ms < 0)
+        s->cv.wait(lk, ready);
+    else if (!s->cv.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready))
+        return tvmc::set_error(TVMC_ERR_TIMEOUT, "request not complete within the timeout");
+    if (r->state == State::Failed) return tvmc::set_error(r->status, r->error.c_str());
+    tvmc_commitment* c = r->c;
+    lk.unlock();
+    if (!c) return tvmc::set_error(TVMC_ERR_CUDA, "request finished without a commitment");
+    return root ? tvmc_commitment_root(c, root) : TVMC_OK;
+}
+
+int tvmc_server_open(tvmc_server* s, uint64_t id, const size_t* leaf_idx, size_t count, uint64_t* paths,
+                     uint64_t* rows) {
+    if (!s) return tvmc::set_error(TVMC_ERR_INVALID, "null server");
+    tvmc_commitment* c = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        Request* r = find(s, id);
+        if (!r) return tvmc::set_error(TVMC_ERR_INVALID, "unknown request id");
+        if (r->state != State::Done || !r->c) return tvmc::set_error(TVMC_ERR_INVALID, "request not committed");
+        if (rows && !s->keep_lde) return tvmc::set_error(TVMC_ERR_INVALID, "server does not keep LDEs");
+        c = r->c;
+    }
+    int rc = paths ? tvmc_commitment_auth_paths(c, leaf_idx, count, paths) : TVMC_OK;
+    if (!rc && rows) rc = tvmc_commitment_read_rows(c, leaf_idx, count, rows);
+    return rc;
+}
+
+int tvmc_server_times(tvmc_server* s, uint64_t id, uint64_t* submit_ns, uint64_t* start_ns, uint64_t* done_ns) {
+    if (!s) return tvmc::set_error(TVMC_ERR_INVALID, "null server");
+    std::lock_guard<std::mutex> lk(s->mu);
+    Request* r = find(s, id);
+    if (!r) return tvmc::set_error(TVMC_ERR_INVALID, "unknown request id");
+    if (submit_ns) *submit_ns = r->t_submit;
+    if (start_ns) *start_ns = r->t_start;
+    if (done_ns) *done_ns = r->t_done;
+    return TVMC_OK;
+}
+
+int tvmc_server_release(tvmc_server* s, uint64_t id) {
+    if (!s) return tvmc::set_error(TVMC_ERR_INVALID, "null server");
+    std::unique_ptr<Request> r;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        auto it = s->reqs.find(id);
+        if (it == s->reqs.end()) return tvmc::set_error(TVMC_ERR_INVALID, "unknown request id");
+        Request* q = it->second.get();
+        if (q->state == State::Queued || q->state == State::Running)
+            return tvmc::set_error(TVMC_ERR_INVALID, "request still in flight; wait for it first");
+        if (q->state == State::Done) s->used -= q->resident;
+        r = std::move(it->second);
+        s->reqs.erase(it);
+        s->released++;
+        s->cv.notify_all();
+    }
+    if (r->c) tvmc_commitment_free(r->c);
+    return TVMC_OK;
+}
+
+int tvmc_server_get_stats(tvmc_server* s, tvmc_server_stats* out) {
+    if (!s || !out) return tvmc::set_error(TVMC_ERR_INVALID, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    out->submitted = s->submitted;
+    out->completed = s->completed;
+    out->failed = s->failed;
+    out->released = s->released;
+    out->queued = s->queue.size();
+    out->running = (uint64_t)s->running;
+    out->bytes_in_use = s->used;
+    out->bytes_peak = s->peak;
+    out->budget = s->budget;
+    return TVMC_OK;
+}
+
+int tvmc_server_destroy(tvmc_server* s) {
+    if (!s) return TVMC_OK;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+        s->cv.notify_all();
+    }
+    s->dispatcher.join();
+    for (auto st : s->streams) cudaStreamSynchronize(st);  // every on_done has run
+    for (auto& kv : s->reqs)
+        if (kv.second->c) tvmc_commitment_free(kv.second->c);
+    for (auto st : s->streams) cudaStreamDestroy(st);
+    delete s;
+    return TVMC_OK;
+}
+
+}  // extern "C"

@@ -48,6 +48,14 @@ class OutOfRange(TvmcError, IndexError):
     pass
 
 
+class Timeout(TvmcError, TimeoutError):
+    pass
+
+
+class OutOfMemory(TvmcError, MemoryError):
+    pass
+
+
 def build() -> None:
     subprocess.run(["make", "-s", "-C", HERE], check=True)
 
@@ -110,6 +118,15 @@ SIGNATURES = {
     "tvmc_batch_run": (ctypes.c_int, [_vp, _vp]),
     "tvmc_batch_commitment": (ctypes.c_int, [_vp, _sz, ctypes.POINTER(_vp)]),
     "tvmc_batch_free": (ctypes.c_int, [_vp]),
+    "tvmc_server_create": (ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),
+    "tvmc_server_submit": (ctypes.c_int, [_vp, _vp, _sz, _sz, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint32,
+                                          ctypes.POINTER(ctypes.c_uint64)]),
+    "tvmc_server_wait": (ctypes.c_int, [_vp, ctypes.c_uint64, ctypes.c_int64, _u64p]),
+    "tvmc_server_open": (ctypes.c_int, [_vp, ctypes.c_uint64, _szp, _sz, _u64p, _u64p]),
+    "tvmc_server_times": (ctypes.c_int, [_vp, ctypes.c_uint64, _u64p, _u64p, _u64p]),
+    "tvmc_server_release": (ctypes.c_int, [_vp, ctypes.c_uint64]),
+    "tvmc_server_get_stats": (ctypes.c_int, [_vp, _vp]),
+    "tvmc_server_destroy": (ctypes.c_int, [_vp]),
     "tvmc_set_tuning": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_longlong]),
     "tvmc_get_tuning": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_longlong)]),
     "tvmc_int_peak_probe": (ctypes.c_double, [_vp]),
@@ -141,6 +158,10 @@ def _check(status: int) -> None:
         raise InvalidArgument(status, msg)
     if status == ERR_RANGE:
         raise OutOfRange(status, msg)
+    if status == ERR_TIMEOUT:
+        raise Timeout(status, msg)
+    if status == ERR_NOMEM:
+        raise OutOfMemory(status, msg)
     raise TvmcError(status, msg)
 
 
@@ -537,3 +558,95 @@ class Batch:
 
     def __exit__(self, *a):
         self.free()
+
+
+SERVER_KEEP_LDE = 0x1
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", ctypes.c_size_t), ("num_streams", ctypes.c_uint32),
+                ("flags", ctypes.c_uint32)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_uint64) for k in ("submitted", "completed", "failed", "released", "queued",
+                                                "running")] + \
+               [(k, ctypes.c_size_t) for k in ("bytes_in_use", "bytes_peak", "budget")]
+
+
+class Server:
+    """Commitment serving loop (tvmc_server_*): HBM-budget admission, requests
+    dispatched over worker streams as they arrive, trees kept on the device
+    for openings until release."""
+
+    def __init__(self, hbm_budget_bytes: int = 0, streams: int = 4, keep_lde: bool = False):
+        cfg = ServerConfig(hbm_budget_bytes, streams, SERVER_KEEP_LDE if keep_lde else 0)
+        h = _vp()
+        _check(lib().tvmc_server_create(ctypes.byref(cfg), ctypes.byref(h)))
+        self.h = h
+        self.keep_lde = keep_lde
+        self._meta = {}  # id -> (height, width, trace buffer kept alive until committed)
+
+    def submit(self, trace, expansion: int = 4, offset: int = 7, row_major: bool = False, frugal: bool = False,
+               width: int | None = None, trace_len: int | None = None, device_ptr: bool = False) -> int:
+        flags = (TRACE_ROW_MAJOR if row_major else 0) | (FRUGAL if frugal else 0)
+        if device_ptr:
+            flags |= TRACE_DEVICE
+            ptr, keep = int(trace), None
+        else:
+            t = _u64(trace)
+            trace_len, width = t.shape if row_major else t.shape[::-1]
+            ptr, keep = (t.ctypes.data if t.size else None), t
+        rid = ctypes.c_uint64(0)
+        _check(lib().tvmc_server_submit(self.h, ptr, trace_len, width, expansion, offset, flags, ctypes.byref(rid)))
+        self._meta[rid.value] = ((trace_len * expansion).bit_length() - 1, width, keep)
+        return rid.value
+
+    def wait(self, rid: int, timeout_ms: int = -1) -> np.ndarray:
+        root = np.zeros(5, dtype=np.uint64)
+        _check(lib().tvmc_server_wait(self.h, rid, timeout_ms, _p(root)))
+        h, w, _ = self._meta[rid]
+        self._meta[rid] = (h, w, None)
+        return root
+
+    def open(self, rid: int, leaves, rows: bool = False):
+        h, w, _ = self._meta[rid]
+        ix = np.ascontiguousarray(leaves, dtype=np.uintp)
+        paths = np.zeros((ix.size, h, 5), dtype=np.uint64)
+        rr = np.zeros((ix.size, w), dtype=np.uint64) if rows else None
+        _check(lib().tvmc_server_open(self.h, rid, ix.ctypes.data_as(_szp), ix.size,
+                                      _p(paths) if paths.size else None,
+                                      _p(rr) if rows and rr.size else None))
+        return (paths, rr) if rows else paths
+
+    def times(self, rid: int):
+        """(submit, start, done) in time.monotonic_ns() nanoseconds."""
+        a, b, c = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        _check(lib().tvmc_server_times(self.h, rid, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return a.value, b.value, c.value
+
+    def release(self, rid: int) -> None:
+        _check(lib().tvmc_server_release(self.h, rid))
+        self._meta.pop(rid, None)
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(lib().tvmc_server_get_stats(self.h, ctypes.byref(st)))
+        return {k: getattr(st, k) for k, _ in ServerStats._fields_}
+
+    def close(self) -> None:
+        if self.h is not None:
+            lib().tvmc_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
