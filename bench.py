@@ -523,31 +523,36 @@ def run_serving(args):
     st = torch.cuda.Stream(dev)
 
     def plain(arr_ns):
-        lat = []
+        lat, svc = [], []
         t0 = time.monotonic_ns() + 20_000_000
         for i, t in enumerate(reqs):
             target = t0 + arr_ns[i]
             while time.monotonic_ns() < target:
                 time.sleep(max(0.0, (target - time.monotonic_ns()) / 1e9 - 0.0005))
+            start = time.monotonic_ns()
             c = tvmc.Commitment(t, stream=st.cuda_stream, discard_lde=True)
             c.root()
-            lat.append(time.monotonic_ns() - target)
+            done = time.monotonic_ns()
+            lat.append(done - target)
+            svc.append(done - start)
             c.auth_paths(opens[i])
             c.free()
-        return lat, (time.monotonic_ns() - t0 - arr_ns[0]) / 1e9
+        return lat, (time.monotonic_ns() - t0 - arr_ns[0]) / 1e9, svc
 
     def served(arr_ns):
-        lat = [0] * M
+        lat, svc = [0] * M, [0] * M
         ids = [None] * M
         ready = [threading.Event() for _ in range(M)]
         t0 = time.monotonic_ns() + 20_000_000
-        with tvmc.Server(streams=args.serve_streams) as srv:
+        with tvmc.Server(streams=args.serve_streams, max_large=args.serve_max_large) as srv:
             def waiter():
                 for i in range(M):
                     ready[i].wait()
                     srv.wait(ids[i])
                     srv.open(ids[i], opens[i])
-                    lat[i] = srv.times(ids[i])[2] - (t0 + arr_ns[i])
+                    _sub, start, done = srv.times(ids[i])
+                    lat[i] = done - (t0 + arr_ns[i])
+                    svc[i] = done - start
                     srv.release(ids[i])
             th = threading.Thread(target=waiter)
             th.start()
@@ -559,17 +564,26 @@ def run_serving(args):
                 ready[i].set()
             th.join()
             stats = srv.stats()
-        return lat, (time.monotonic_ns() - t0 - arr_ns[0]) / 1e9, stats
+        return lat, (time.monotonic_ns() - t0 - arr_ns[0]) / 1e9, stats, svc
 
-    def summ(lat, span):
+    large = np.array([c * 8 > (128 << 20) for c in cells])
+
+    def summ(lat, span, svc):
         ms = np.array(lat) / 1e6
-        return {"p50_ms": float(np.percentile(ms, 50)), "p99_ms": float(np.percentile(ms, 99)),
-                "mean_ms": float(ms.mean()), "throughput_rps": M / span, "cells_per_s": sum(cells) / span}
+        sv = np.array(svc) / 1e6
+        out = {"p50_ms": float(np.percentile(ms, 50)), "p99_ms": float(np.percentile(ms, 99)),
+               "mean_ms": float(ms.mean()), "throughput_rps": M / span, "cells_per_s": sum(cells) / span}
+        for name, sel in (("small", ~large), ("large", large)):
+            if sel.any():
+                out[f"{name}_p50_ms"] = float(np.percentile(ms[sel], 50))
+                out[f"{name}_p99_ms"] = float(np.percentile(ms[sel], 99))
+                out[f"{name}_service_mean_ms"] = float(sv[sel].mean())
+        return out
 
     zero = [0] * M
     plain(zero)  # warm-up: twiddle tables, pool, pinned paths
     served(zero)
-    lat0, span0 = plain(zero)  # back-to-back: the plain path's service time
+    lat0, span0, _ = plain(zero)  # back-to-back: the plain path's service time
     service_s = span0 / M
     rates = []
     for rho in args.serve_loads:
@@ -577,15 +591,17 @@ def run_serving(args):
         gaps = np.random.default_rng(int(rho * 1000)).exponential(1.0 / lam, M)
         arr = (np.cumsum(gaps) - gaps[0]) * 1e9
         arr_ns = [int(x) for x in arr]
-        pl, pspan = plain(arr_ns)
-        sv, sspan, stats = served(arr_ns)
-        rates.append({"load_vs_plain_capacity": rho, "rate_rps": lam, "plain": summ(pl, pspan),
-                      "server": summ(sv, sspan), "server_peak_bytes": stats["bytes_peak"],
+        pl, pspan, psvc = plain(arr_ns)
+        sv, sspan, stats, ssvc = served(arr_ns)
+        rates.append({"load_vs_plain_capacity": rho, "rate_rps": lam, "plain": summ(pl, pspan, psvc),
+                      "server": summ(sv, sspan, ssvc), "server_peak_bytes": stats["bytes_peak"],
                       "server_budget_bytes": stats["budget"]})
     line = {"metric": "serving latency p50/p99 and throughput", "workload": "serving", "requests": M,
             "plain_service_ms_mean": 1e3 * service_s,
             "config": {"heights": f"2^10..2^{args.serve_max_log_n} log-uniform", "widths": [W_MAIN, W_AUX],
                        "expansion": EXPANSION, "openings_per_request": 80, "server_streams": args.serve_streams,
+                       "server_max_large_inflight": args.serve_max_large,
+                       "small_large_split": "LDE <= 128 MB is small",
                        "host_buffers": "pinned, one per (height, width) class",
                        "latency": "arrival -> root committed (server: completion callback time)"},
             "rates": rates, "n_gpus": 1, "data": "synthetic uniform field elements"}
@@ -607,6 +623,7 @@ def main():
     ap.add_argument("--requests", type=int, default=48, help="serving: requests per rate")
     ap.add_argument("--serve-streams", type=int, default=4)
     ap.add_argument("--serve-max-log-n", type=int, default=20)
+    ap.add_argument("--serve-max-large", type=int, default=1, help="serving: large tables committed at once")
     ap.add_argument("--serve-loads", type=float, nargs="+", default=[0.5, 0.9, 1.5, 3.0],
                     help="serving: offered load as a multiple of the plain path's capacity")
     args = ap.parse_args()

@@ -295,8 +295,11 @@ int tvmc_batch_free(tvmc_batch* b);
  * in arrival order; the head is admitted as soon as its device footprint
  * (tree, LDE, LDE scratch, upload staging) fits the HBM budget beside the
  * running requests and the trees still held, and is issued at once on the
- * least-loaded of its worker streams (small tables on high-priority streams),
- * so requests of mixed sizes run concurrently as they arrive.  Each request's
+ * least-loaded of its worker streams.  Small tables (LDE up to 128 MB) run
+ * concurrently on num_streams high-priority streams and never wait behind
+ * large ones; large tables, each enough to fill the GPU, run
+ * max_large_inflight at a time in arrival order, each slot with its own
+ * stream.  Each request's
  * Merkle tree stays on the device for openings until tvmc_server_release;
  * with TVMC_SERVER_KEEP_LDE its LDE stays too (rows can be opened).  Results
  * are bit-identical to tvmc_commit of the same table alone.  The trace buffer
@@ -308,8 +311,9 @@ typedef struct tvmc_server tvmc_server;
 
 typedef struct tvmc_server_config {
     size_t hbm_budget_bytes; /* 0: 90% of the device memory free at creation */
-    uint32_t num_streams;    /* worker streams, 0: 4 (at most 64) */
+    uint32_t num_streams;    /* worker streams for small tables, 0: 4 (at most 64) */
     uint32_t flags;          /* TVMC_SERVER_KEEP_LDE */
+    uint32_t max_large_inflight; /* large tables committed at once, 0: 1 (at most 16) */
 } tvmc_server_config;
 
 typedef struct tvmc_server_stats {

@@ -262,18 +262,22 @@ int run_lde(const LdePlan& pl, const uint64_t* d_tr, uint64_t tld, uint64_t* d_o
 }
 
 // Per-device non-blocking stream for host->device uploads.
-std::map<int, cudaStream_t> g_copy_streams;
+// One non-blocking upload stream per (device, compute stream): the uploads of
+// a commit wait on its own compute stream's progress, so commits issued on
+// different streams never queue behind each other's uploads.
+std::map<std::pair<int, cudaStream_t>, cudaStream_t> g_copy_streams;
 
-int copy_stream(cudaStream_t* out) {
+int copy_stream(cudaStream_t compute, cudaStream_t* out) {
     int dev;
     int rc = current_device(&dev);
     if (rc) return rc;
     std::lock_guard<std::mutex> lk(g_mu);
-    auto it = g_copy_streams.find(dev);
+    auto key = std::make_pair(dev, compute);
+    auto it = g_copy_streams.find(key);
     if (it == g_copy_streams.end()) {
         cudaStream_t s;
         CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-        it = g_copy_streams.emplace(dev, s).first;
+        it = g_copy_streams.emplace(key, s).first;
     }
     *out = it->second;
     return TVMC_OK;
@@ -285,7 +289,7 @@ int copy_stream(cudaStream_t* out) {
 int upload_lde_pipelined(const LdePlan& pl, const uint64_t* h_trace, size_t n, size_t width, uint64_t* d_out,
                          size_t L, cudaStream_t st, const RandAdd& ra = RandAdd{}) {
     cudaStream_t cs = nullptr;
-    int rc = copy_stream(&cs);
+    int rc = copy_stream(st, &cs);
     if (rc) return rc;
     size_t chunk = lde_chunk_cols(pl.logn, pl.log_exp, width);
     // keep staging chunks near 256 MB so the first upload is short

@@ -1,11 +1,16 @@
 // Commitment serving runtime (host C++; the GPU work is tvmc_commit's).
 //
 // A server owns worker streams on one device and a dispatcher thread.
-// Submitted requests queue in arrival order; the dispatcher admits the head of
-// the queue as soon as its device footprint fits the HBM budget next to what
-// running requests and resident trees already hold, and issues it at once on
-// the least-loaded worker stream (small tables on high-priority streams), so
-// requests of mixed sizes run concurrently as they arrive.  A host callback
+// Submitted requests queue in arrival order, in two classes: large tables
+// (LDE above 128 MB, enough work to fill the GPU alone) and small ones.  The
+// dispatcher admits a queue head as soon as its device footprint fits the HBM
+// budget next to what running requests and resident trees already hold --
+// small tables at once, on high-priority worker streams, and large tables up
+// to a limit in flight (default 1: two GPU-filling commits only share the
+// GPU), each on its own dedicated stream, so that the stream-ordered memory
+// pool hands a large commit's multi-GB buffers straight to the next one --
+// so small requests never wait behind large ones and requests of mixed sizes
+// overlap as they arrive.  A host callback
 // on the stream marks each request done, records its completion time and
 // returns its transient memory to the budget; its Merkle tree (and, with
 // TVMC_SERVER_KEEP_LDE, its LDE) stays on the device for openings until the
@@ -45,6 +50,7 @@ struct Request {
     uint32_t expansion = 4, flags = 0;
     uint64_t offset = 7;
     size_t resident = 0, transient = 0;  // budget bytes held until release / until done
+    bool large = false;
     int stream = -1;
     State state = State::Queued;
     int status = TVMC_OK;
@@ -68,6 +74,7 @@ void footprint(Request* r, bool keep_lde, size_t scratch_budget) {
     else upload = (dev ? 0 : NW) + (rm ? NW : 0);
     r->resident = tree + (keep_lde && !frugal ? lde : 0);
     r->transient = (keep_lde && !frugal ? 0 : lde) + scratch + upload;
+    r->large = L * std::max<size_t>(W, 1) * 8 > (size_t(128) << 20);
 }
 
 }  // namespace
@@ -77,11 +84,13 @@ struct tvmc_server {
     size_t budget = 0;
     bool keep_lde = false;
     size_t scratch_budget = size_t(2) << 30;
-    std::vector<cudaStream_t> streams;
-    std::vector<int> inflight;  // per stream
+    std::vector<cudaStream_t> streams;  // [0, n_small): small tables; the rest: one per large slot
+    std::vector<int> inflight;          // per stream
+    int n_small = 0;
     std::mutex mu;
     std::condition_variable cv;  // queue changes, completions, releases
-    std::deque<Request*> queue;
+    std::deque<Request*> queue_small, queue_large;
+    int max_large = 1, large_running = 0;
     std::unordered_map<uint64_t, std::unique_ptr<Request>> reqs;
     size_t used = 0, peak = 0;
     uint64_t next_id = 1, submitted = 0, completed = 0, failed = 0, released = 0;
@@ -107,6 +116,7 @@ void CUDART_CB on_done(void* p) {
     s->used -= r->transient;
     s->inflight[r->stream]--;
     s->running--;
+    if (r->large) s->large_running--;
     s->completed++;
     s->cv.notify_all();
 }
@@ -120,19 +130,28 @@ void fail_request(tvmc_server* s, Request* r, int status, const std::string& msg
     s->cv.notify_all();
 }
 
+// The next request to issue: a small head that fits, else a large head that
+// fits under the in-flight limit, else a head that can never fit (to fail it).
+Request* pick(tvmc_server* s) {
+    auto fits = [&](Request* r) { return s->used + r->resident + r->transient <= s->budget; };
+    auto never = [&](Request* r) { return r->resident + r->transient > s->budget; };
+    if (!s->queue_small.empty() && (fits(s->queue_small.front()) || never(s->queue_small.front())))
+        return s->queue_small.front();
+    if (!s->queue_large.empty()) {
+        Request* r = s->queue_large.front();
+        if (never(r) || (s->large_running < s->max_large && fits(r))) return r;
+    }
+    return nullptr;
+}
+
 void dispatch_loop(tvmc_server* s) {
     cudaSetDevice(s->device);
     std::unique_lock<std::mutex> lk(s->mu);
     while (true) {
-        s->cv.wait(lk, [&] {
-            if (s->stop) return true;
-            if (s->queue.empty()) return false;
-            Request* r = s->queue.front();
-            return r->resident + r->transient > s->budget || s->used + r->resident + r->transient <= s->budget;
-        });
+        Request* r = nullptr;
+        s->cv.wait(lk, [&] { return s->stop || (r = pick(s)) != nullptr; });
         if (s->stop) return;
-        Request* r = s->queue.front();
-        s->queue.pop_front();
+        (r->large ? s->queue_large : s->queue_small).pop_front();
         const size_t need = r->resident + r->transient;
         if (need > s->budget) {
             fail_request(s, r, TVMC_ERR_NOMEM, "request footprint exceeds the server's HBM budget");
@@ -140,17 +159,14 @@ void dispatch_loop(tvmc_server* s) {
         }
         s->used += need;
         s->peak = std::max(s->peak, s->used);
-        // small tables to the high-priority half of the streams
-        const bool small = r->n * r->expansion * std::max<size_t>(r->width, 1) <= (size_t(1) << 22);
-        const int half = (int)s->streams.size() / 2;
-        int lo = small ? 0 : half, hi = small ? half : (int)s->streams.size();
-        if (lo == hi) lo = 0, hi = (int)s->streams.size();
+        const int lo = r->large ? s->n_small : 0, hi = r->large ? (int)s->streams.size() : s->n_small;
         int best = lo;
         for (int i = lo; i < hi; i++)
             if (s->inflight[i] < s->inflight[best]) best = i;
         r->stream = best;
         s->inflight[best]++;
         s->running++;
+        if (r->large) s->large_running++;
         r->state = State::Running;
         r->t_start = now_ns();
         const uint32_t flags = (r->flags & (TVMC_TRACE_DEVICE | TVMC_TRACE_ROW_MAJOR | TVMC_FRUGAL)) |
@@ -161,10 +177,14 @@ void dispatch_loop(tvmc_server* s) {
         const int rc = tvmc_commit(r->trace, r->n, r->width, r->expansion, r->offset, flags, st, &c);
         const std::string err = rc ? tvmc_last_error() : "";
         lk.lock();
-        if (rc) {
+        auto undo = [&] {
             s->used -= need;
             s->inflight[best]--;
             s->running--;
+            if (r->large) s->large_running--;
+        };
+        if (rc) {
+            undo();
             fail_request(s, r, rc, err);
             continue;
         }
@@ -176,9 +196,7 @@ void dispatch_loop(tvmc_server* s) {
         if (e != cudaSuccess) {
             delete ctx;
             r->c = nullptr;
-            s->used -= need;
-            s->inflight[best]--;
-            s->running--;
+            undo();
             fail_request(s, r, TVMC_ERR_CUDA, cudaGetErrorString(e));
             lk.unlock();
             tvmc_commitment_free(c);
@@ -210,14 +228,17 @@ int tvmc_server_create(const tvmc_server_config* cfg, tvmc_server** out) {
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return tvmc::set_error(TVMC_ERR_CUDA, "cudaMemGetInfo");
     s->budget = c.hbm_budget_bytes ? c.hbm_budget_bytes : free_b / 10 * 9;
     s->keep_lde = c.flags & TVMC_SERVER_KEEP_LDE;
+    s->max_large = c.max_large_inflight ? (int)c.max_large_inflight : 1;
     long long sb = 0;
     if (tvmc_get_tuning("lde_scratch_bytes", &sb) == TVMC_OK && sb > 0) s->scratch_budget = (size_t)sb;
-    const int ns = c.num_streams ? (int)std::min<uint32_t>(c.num_streams, 64) : 4;
+    s->n_small = c.num_streams ? (int)std::min<uint32_t>(c.num_streams, 64) : 4;
+    s->max_large = (int)std::min<uint32_t>(s->max_large, 16);
+    const int ns = s->n_small + s->max_large;
     int lo_prio = 0, hi_prio = 0;
     cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio);
     for (int i = 0; i < ns; i++) {
         cudaStream_t st;
-        const int prio = (ns > 1 && i < ns / 2) ? hi_prio : lo_prio;
+        const int prio = i < s->n_small ? hi_prio : lo_prio;
         if (cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, prio) != cudaSuccess) {
             for (auto x : s->streams) cudaStreamDestroy(x);
             return tvmc::set_error(TVMC_ERR_CUDA, "cannot create worker streams");
@@ -253,7 +274,7 @@ int tvmc_server_submit(tvmc_server* s, const uint64_t* trace, size_t trace_len, 
     footprint(r.get(), s->keep_lde, s->scratch_budget);
     r->id = s->next_id++;
     *id = r->id;
-    s->queue.push_back(r.get());
+    (r->large ? s->queue_large : s->queue_small).push_back(r.get());
     s->reqs.emplace(r->id, std::move(r));
     s->submitted++;
     s->cv.notify_all();
@@ -332,7 +353,7 @@ int tvmc_server_get_stats(tvmc_server* s, tvmc_server_stats* out) {
     out->completed = s->completed;
     out->failed = s->failed;
     out->released = s->released;
-    out->queued = s->queue.size();
+    out->queued = s->queue_small.size() + s->queue_large.size();
     out->running = (uint64_t)s->running;
     out->bytes_in_use = s->used;
     out->bytes_peak = s->peak;

@@ -565,7 +565,7 @@ SERVER_KEEP_LDE = 0x1
 
 class ServerConfig(ctypes.Structure):
     _fields_ = [("hbm_budget_bytes", ctypes.c_size_t), ("num_streams", ctypes.c_uint32),
-                ("flags", ctypes.c_uint32)]
+                ("flags", ctypes.c_uint32), ("max_large_inflight", ctypes.c_uint32)]
 
 
 class ServerStats(ctypes.Structure):
@@ -579,8 +579,8 @@ class Server:
     dispatched over worker streams as they arrive, trees kept on the device
     for openings until release."""
 
-    def __init__(self, hbm_budget_bytes: int = 0, streams: int = 4, keep_lde: bool = False):
-        cfg = ServerConfig(hbm_budget_bytes, streams, SERVER_KEEP_LDE if keep_lde else 0)
+    def __init__(self, hbm_budget_bytes: int = 0, streams: int = 4, keep_lde: bool = False, max_large: int = 0):
+        cfg = ServerConfig(hbm_budget_bytes, streams, SERVER_KEEP_LDE if keep_lde else 0, max_large)
         h = _vp()
         _check(lib().tvmc_server_create(ctypes.byref(cfg), ctypes.byref(h)))
         self.h = h
