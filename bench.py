@@ -59,6 +59,25 @@ def perms_per_table(L: int, width: int) -> int:
     return L * (width // 10 + 1) + (L - 1)
 
 
+def max_over_ranks(x: float, device=None) -> float:
+    """The maximum of x over all ranks (the job's time is its slowest rank's);
+    x itself when not distributed.  device: where the collective's tensor lives
+    (a CUDA device under NCCL, None = CPU under gloo)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return x
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(units_per_rank: float, ranks: int, seconds_max: float) -> float:
+    """Replicas (weak scaling): every rank processes units_per_rank; the job
+    takes the slowest rank's time."""
+    return ranks * units_per_rank / seconds_max
+
+
 def dist_info():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -278,13 +297,8 @@ def run_ours(args):
     launches = tvmc.lib().tvmc_launch_count() - launches0
     t_ms = ev0.elapsed_time(ev1)
     barrier()
-    t_max = t_ms
-    if ws > 1:
-        import torch.distributed as dist
-        tt = torch.tensor([t_ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt.item())
-    value = ws * cells_step * args.steps / (t_max / 1e3)
+    t_max = max_over_ranks(t_ms, dev)
+    value = whole_job_rate(cells_step * args.steps, ws, t_max / 1e3)
 
     # dominant kernel: Tip5 row hash + tree (phase 3); LDE phase against HBM
     hash_ms = [p[2] for p in phases]
@@ -333,13 +347,8 @@ def run_ours(args):
         for _ in range(args.steps):
             e2e_step()
         torch.cuda.synchronize()
-        te = time.perf_counter() - t0
-        if ws > 1:
-            import torch.distributed as dist
-            tt = torch.tensor([te], device=dev, dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            te = float(tt.item())
-        e2e = {"value": ws * cells_step * args.steps / te, "unit": "cells/s",
+        te = max_over_ranks(time.perf_counter() - t0, dev)
+        e2e = {"value": whole_job_rate(cells_step * args.steps, ws, te), "unit": "cells/s",
                "h2d_bytes_per_step": 8 * n * (W_MAIN + W_AUX), "d2h_bytes_per_step": 2 * 40,
                "ms_per_step": 1e3 * te / args.steps}
 
