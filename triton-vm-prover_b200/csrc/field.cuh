@@ -14,7 +14,28 @@ namespace tvmc {
 constexpr uint64_t GL_P = 0xFFFFFFFF00000001ull;
 constexpr uint64_t GL_EPS = 0xFFFFFFFFull;  // 2^64 mod p
 
-__device__ __forceinline__ uint64_t gl_canon(uint64_t a) { return a >= GL_P ? a - GL_P : a; }
+// The add/sub/canonicalisation helpers below are 32-bit carry chains: a >= p
+// exactly when a + (2^32 - 1) carries out of 64 bits, so the comparison is the
+// carry of the correction itself (no separate compares), and a borrow becomes
+// an all-ones mask that subtracts 2^32 - 1 (adds p) directly.
+
+// Canonical representative of any 64-bit value.
+__device__ __forceinline__ uint64_t gl_canon(uint64_t a) {
+    uint32_t r0, r1;
+    asm("{\n\t"
+        ".reg .u32 t0, t1, c;\n\t"
+        ".reg .pred q;\n\t"
+        "add.cc.u32 t0, %2, 0xFFFFFFFF;\n\t"
+        "addc.cc.u32 t1, %3, 0;\n\t"
+        "addc.u32 c, 0, 0;\n\t"
+        "setp.ne.u32 q, c, 0;\n\t"
+        "selp.b32 %0, t0, %2, q;\n\t"
+        "selp.b32 %1, t1, %3, q;\n\t"
+        "}"
+        : "=r"(r0), "=r"(r1)
+        : "r"((uint32_t)a), "r"((uint32_t)(a >> 32)));
+    return ((uint64_t)r1 << 32) | r0;
+}
 
 // (hi:lo) -> a 64-bit representative (not necessarily < p) of the residue.
 __device__ __forceinline__ uint64_t gl_reduce128(uint64_t lo, uint64_t hi) {
@@ -81,23 +102,62 @@ __device__ __forceinline__ uint64_t gl_mul_c(uint64_t a, uint64_t b) { return gl
 
 __device__ __forceinline__ uint64_t gl_sqr(uint64_t a) { return gl_mul(a, a); }
 
-// a + b where b < p (a any representative); partial result.
+// a + b where b < p (a any representative); partial result.  A carry out of
+// 64 bits means the sum exceeds 2^64 by less than p, so adding 2^32 - 1 (i.e.
+// subtracting p modulo 2^64) cannot carry again.
 __device__ __forceinline__ uint64_t gl_add_pc(uint64_t a, uint64_t b) {
-    uint64_t s = a + b;
-    if (s < b) s += GL_EPS;
-    return s;
+    uint32_t r0, r1;
+    asm("{\n\t"
+        ".reg .u32 s0, s1, m;\n\t"
+        "add.cc.u32 s0, %2, %4;\n\t"
+        "addc.cc.u32 s1, %3, %5;\n\t"
+        "addc.u32 m, 0, 0;\n\t"
+        "neg.s32 m, m;\n\t"
+        "add.cc.u32 %0, s0, m;\n\t"
+        "addc.u32 %1, s1, 0;\n\t"
+        "}"
+        : "=r"(r0), "=r"(r1)
+        : "r"((uint32_t)a), "r"((uint32_t)(a >> 32)), "r"((uint32_t)b), "r"((uint32_t)(b >> 32)));
+    return ((uint64_t)r1 << 32) | r0;
 }
 
-// Canonical add / sub of canonical operands.
+// Canonical add of canonical operands: s = a + b (65 bits); s - p is s + 2^32 - 1
+// modulo 2^64, taken when either addition carries.
 __device__ __forceinline__ uint64_t gl_add_c(uint64_t a, uint64_t b) {
-    uint64_t s = a + b;
-    if (s < a || s >= GL_P) s -= GL_P;
-    return s;
+    uint32_t r0, r1;
+    asm("{\n\t"
+        ".reg .u32 s0, s1, t0, t1, c;\n\t"
+        ".reg .pred q;\n\t"
+        "add.cc.u32 s0, %2, %4;\n\t"
+        "addc.cc.u32 s1, %3, %5;\n\t"
+        "addc.u32 c, 0, 0;\n\t"
+        "add.cc.u32 t0, s0, 0xFFFFFFFF;\n\t"
+        "addc.cc.u32 t1, s1, 0;\n\t"
+        "addc.u32 c, c, 0;\n\t"
+        "setp.ne.u32 q, c, 0;\n\t"
+        "selp.b32 %0, t0, s0, q;\n\t"
+        "selp.b32 %1, t1, s1, q;\n\t"
+        "}"
+        : "=r"(r0), "=r"(r1)
+        : "r"((uint32_t)a), "r"((uint32_t)(a >> 32)), "r"((uint32_t)b), "r"((uint32_t)(b >> 32)));
+    return ((uint64_t)r1 << 32) | r0;
 }
+
+// Canonical sub of canonical operands: on a borrow the wrapped difference is at
+// least 2^32, so subtracting 2^32 - 1 (adding p modulo 2^64) cannot borrow again.
 __device__ __forceinline__ uint64_t gl_sub_c(uint64_t a, uint64_t b) {
-    uint64_t d = a - b;
-    if (a < b) d += GL_P;
-    return d;
+    uint32_t r0, r1;
+    asm("{\n\t"
+        ".reg .u32 s0, s1, m;\n\t"
+        "sub.cc.u32 s0, %2, %4;\n\t"
+        "subc.cc.u32 s1, %3, %5;\n\t"
+        "subc.u32 m, 0, 0;\n\t"
+        "sub.cc.u32 %0, s0, m;\n\t"
+        "subc.u32 %1, s1, 0;\n\t"
+        "}"
+        : "=r"(r0), "=r"(r1)
+        : "r"((uint32_t)a), "r"((uint32_t)(a >> 32)), "r"((uint32_t)b), "r"((uint32_t)(b >> 32)));
+    return ((uint64_t)r1 << 32) | r0;
 }
 
 __device__ __forceinline__ uint64_t gl_pow(uint64_t b, uint64_t e) {
