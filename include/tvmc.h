@@ -209,6 +209,12 @@ typedef struct tvmc_commitment tvmc_commitment;
  *                         eight inside the row-hash CTAs; default 0
  * Unknown keys return TVMC_ERR_INVALID. */
 int tvmc_set_tuning(const char* key, long long value);
+/* The library keeps its LDE/NTT scratch and upload staging per (device, stream)
+ * once used, and the device's stream-ordered memory pool keeps freed memory, so
+ * that repeated commits never wait for the driver to map memory.  This frees
+ * that scratch and returns the pool's unused memory on the current device; it
+ * synchronizes the device first. */
+int tvmc_release_cached_memory(void);
 int tvmc_get_tuning(const char* key, long long* value);
 
 /* Commit to one table: LDE of every column onto offset * <w_{trace_len*expansion}>

@@ -242,22 +242,47 @@ int build_rand_add(const uint64_t* d_r, size_t R, size_t width, int logn, int le
 // Coset offset of the LDE plan for trace offset t and evaluation offset o: o / t.
 uint64_t plan_offset(uint64_t t, uint64_t o) { return hmul(o % P, hinv(t % P)); }
 
+// LDE/NTT scratch kept per (device, stream) and grown on demand.  Work issued
+// on one stream runs in order on the GPU, so commits on a stream can share it,
+// and repeated commits allocate no scratch at all: a fresh allocation that had
+// to grow the memory pool would stall the host (and the stream behind it)
+// while the driver maps memory.  tvmc_release_cached_memory frees them.
+struct ScratchSlot {
+    uint64_t* p = nullptr;
+    size_t words = 0;
+};
+// kind: 0 = LDE/NTT intermediates, 1 and 2 = the two upload staging buffers.
+std::map<std::tuple<int, cudaStream_t, int>, ScratchSlot> g_scratch;  // guarded by g_mu
+
+int stream_scratch(cudaStream_t st, size_t words, uint64_t** out, int kind = 0) {
+    *out = nullptr;
+    if (words == 0) return TVMC_OK;
+    int dev;
+    CK(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(g_mu);
+    ScratchSlot& slot = g_scratch[{dev, st, kind}];
+    if (slot.words < words) {
+        if (slot.p) cudaFreeAsync(slot.p, st);  // ordered after the work that used it
+        slot = ScratchSlot{};
+        CK(cudaMallocAsync((void**)&slot.p, words * 8, st));
+        slot.words = words;
+    }
+    *out = slot.p;
+    return TVMC_OK;
+}
+
 int run_lde(const LdePlan& pl, const uint64_t* d_tr, uint64_t tld, uint64_t* d_out, uint64_t old, size_t width,
             cudaStream_t st, const RandAdd& ra = RandAdd{}) {
     size_t chunk = lde_chunk_cols(pl.logn, pl.log_exp, width);
-    size_t sw = lde_scratch_words(pl.logn, pl.log_exp, chunk);
     uint64_t* scratch = nullptr;
-    if (sw) CK(cudaMallocAsync((void**)&scratch, sw * 8, st));
+    int rc = stream_scratch(st, lde_scratch_words(pl.logn, pl.log_exp, chunk), &scratch);
+    if (rc) return rc;
     for (size_t c0 = 0; c0 < width; c0 += chunk) {
         size_t nc = std::min(chunk, width - c0);
         cudaError_t e =
             launch_lde(pl, d_tr + c0 * tld, tld, d_out + c0 * old, old, nc, scratch, st, ra.cols(c0), ra.rm);
-        if (e != cudaSuccess) {
-            if (scratch) cudaFreeAsync(scratch, st);
-            return cuda_fail(e, "launch_lde");
-        }
+        if (e != cudaSuccess) return cuda_fail(e, "launch_lde");
     }
-    if (scratch) CK(cudaFreeAsync(scratch, st));
     return TVMC_OK;
 }
 
@@ -296,13 +321,12 @@ int upload_lde_pipelined(const LdePlan& pl, const uint64_t* h_trace, size_t n, s
     size_t stage_cols = std::max<size_t>(1, (size_t(256) << 20) / (n * 8));
     chunk = std::min(chunk, stage_cols);
     const size_t nchunks = (width + chunk - 1) / chunk;
-    const size_t sw = lde_scratch_words(pl.logn, pl.log_exp, chunk);
     uint64_t *scratch = nullptr, *stage[2] = {nullptr, nullptr};
     cudaEvent_t ready[2] = {nullptr, nullptr}, freed[2] = {nullptr, nullptr};
+    if ((rc = stream_scratch(st, lde_scratch_words(pl.logn, pl.log_exp, chunk), &scratch))) return rc;
     cudaError_t e = cudaSuccess;
-    if (sw) e = cudaMallocAsync((void**)&scratch, sw * 8, st);
     for (int b = 0; b < 2 && e == cudaSuccess; b++) {
-        e = cudaMallocAsync((void**)&stage[b], chunk * n * 8, st);
+        if (stream_scratch(st, chunk * n, &stage[b], 1 + b)) e = cudaErrorMemoryAllocation;
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ready[b], cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&freed[b], cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaEventRecord(freed[b], st);  // allocations are ordered on st
@@ -319,11 +343,9 @@ int upload_lde_pipelined(const LdePlan& pl, const uint64_t* h_trace, size_t n, s
         if (e == cudaSuccess) e = cudaEventRecord(freed[b], st);
     }
     for (int b = 0; b < 2; b++) {
-        if (stage[b]) cudaFreeAsync(stage[b], st);
         if (ready[b]) cudaEventDestroy(ready[b]);  // destruction is deferred until the event completes
         if (freed[b]) cudaEventDestroy(freed[b]);
     }
-    if (scratch) cudaFreeAsync(scratch, st);
     if (e != cudaSuccess) return cuda_fail(e, "pipelined upload/LDE");
     return TVMC_OK;
 }
@@ -348,11 +370,9 @@ int ntt_impl(uint64_t* d, size_t n, size_t cols, int inverse, cudaStream_t st) {
     LdePlan pl;
     int rc = get_plan(l, -1, 0, &pl);
     if (rc) return rc;
-    size_t sw = ntt_scratch_words(l, cols);
     uint64_t* scratch = nullptr;
-    if (sw) CK(cudaMallocAsync((void**)&scratch, sw * 8, st));
+    if ((rc = stream_scratch(st, ntt_scratch_words(l, cols), &scratch))) return rc;
     cudaError_t e = launch_ntt(pl, inverse, d, n, cols, scratch, st);
-    if (scratch) cudaFreeAsync(scratch, st);
     if (e != cudaSuccess) return cuda_fail(e, "launch_ntt");
     return TVMC_OK;
 }
@@ -454,10 +474,10 @@ int commit_frugal(const LdePlan& pl, const uint64_t* trace, bool dev, bool rm, s
     sc = std::max<size_t>(10, sc / 10 * 10);
     const size_t stripe_cols = std::min(sc, std::max<size_t>(width, 1));
     const size_t chunk = std::min(lde_chunk_cols(pl.logn, pl.log_exp, stripe_cols), stripe_cols);
-    const size_t sw = lde_scratch_words(pl.logn, pl.log_exp, chunk);
     if (e == cudaSuccess) e = cudaMallocAsync((void**)&cap, 6 * L * 8, st);
     if (e == cudaSuccess && width) e = cudaMallocAsync((void**)&stripe, stripe_cols * L * 8, st);
-    if (e == cudaSuccess && sw) e = cudaMallocAsync((void**)&scratch, sw * 8, st);
+    if (e == cudaSuccess && stream_scratch(st, lde_scratch_words(pl.logn, pl.log_exp, chunk), &scratch))
+        e = cudaErrorMemoryAllocation;
     size_t c0 = 0;
     bool first = true;
     while (e == cudaSuccess) {
@@ -472,7 +492,7 @@ int commit_frugal(const LdePlan& pl, const uint64_t* trace, bool dev, bool rm, s
         c0 += nc;
         if (last) break;
     }
-    for (uint64_t* p : {up, cm, cap, stripe, scratch})
+    for (uint64_t* p : {up, cm, cap, stripe})
         if (p) cudaFreeAsync(p, st);
     if (prof) cudaEventRecord(prof[2], st);
     if (e != cudaSuccess) return cuda_fail(e, "frugal commit");
@@ -616,6 +636,27 @@ const char* tvmc_status_string(int s) {
 int tvmc_version(void) { return 1; }
 
 unsigned long long tvmc_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
+int tvmc_release_cached_memory(void) {
+    int dev;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceSynchronize());
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        for (auto it = g_scratch.begin(); it != g_scratch.end();) {
+            if (std::get<0>(it->first) == dev) {
+                if (it->second.p) cudaFree(it->second.p);
+                it = g_scratch.erase(it);
+            } else {
+                ++it;
+            }
+        }
+    }
+    cudaMemPool_t pool;
+    CK(cudaDeviceGetDefaultMemPool(&pool, dev));
+    CK(cudaMemPoolTrimTo(pool, 0));
+    return TVMC_OK;
+}
 
 int tvmc_set_tuning(const char* key, long long value) {
     if (!key) return fail(TVMC_ERR_INVALID, "null tuning key");

@@ -118,6 +118,7 @@ SIGNATURES = {
     "tvmc_batch_run": (ctypes.c_int, [_vp, _vp]),
     "tvmc_batch_commitment": (ctypes.c_int, [_vp, _sz, ctypes.POINTER(_vp)]),
     "tvmc_batch_free": (ctypes.c_int, [_vp]),
+    "tvmc_release_cached_memory": (ctypes.c_int, []),
     "tvmc_server_create": (ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),
     "tvmc_server_submit": (ctypes.c_int, [_vp, _vp, _sz, _sz, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint32,
                                           ctypes.POINTER(ctypes.c_uint64)]),
@@ -277,6 +278,11 @@ def merkle_heap(leaves) -> np.ndarray:
 
 def set_tuning(key: str, value: int) -> None:
     _check(lib().tvmc_set_tuning(key.encode(), int(value)))
+
+
+def release_cached_memory() -> None:
+    """Free the per-stream scratch and trim the device pool (synchronizes)."""
+    _check(lib().tvmc_release_cached_memory())
 
 
 def get_tuning(key: str) -> int:
