@@ -57,61 +57,30 @@ __device__ __forceinline__ void gl_mul128(uint64_t a, uint64_t b, uint32_t& r0, 
         : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
 }
 
-// (r3:r2:r1:r0) -> (r1:r0) - r3 + r2*(2^32-1) (mod p) as a 64-bit representative.
+// (r3:r2:r1:r0) -> (r1:r0) + r2*(2^32-1) - r3 (mod p) as a 64-bit
+// representative (2^64 = 2^32 - 1 and 2^96 = -1 mod p).  The first sum is two
+// multiply-adds (on the FMA pipe) with carry c in {0, 1}; subtracting r3 leaves
+// c in {-1, 0, 1}; c*2^64 is folded back as c*(2^32 - 1), which cannot wrap:
+// for c = 1 the low 64 bits are at most 2^64 - 2^33, for c = -1 at least
+// 2^64 - 2^32 + 1.
 __device__ __forceinline__ uint64_t gl_reduce_limbs(uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3) {
     uint32_t x0, x1;
     asm("{\n\t"
-        ".reg .u32 z, t0, t1, bm, u0, u1, cm;\n\t"
-        "mov.u32 z, 0;\n\t"
-        "sub.cc.u32 t0, %2, %5;\n\t"    // t = (r1:r0) - r3
-        "subc.cc.u32 t1, %3, z;\n\t"
-        "subc.u32 bm, z, z;\n\t"        // borrow mask
-        "sub.cc.u32 t0, t0, bm;\n\t"    // borrow: t -= 2^32 - 1 (i.e. + p)
-        "subc.u32 t1, t1, z;\n\t"
-        "sub.cc.u32 u0, z, %4;\n\t"     // u = r2*(2^32 - 1) = (r2 << 32) - r2
-        "subc.u32 u1, %4, z;\n\t"
-        "add.cc.u32 %0, t0, u0;\n\t"    // x = t + u
-        "addc.cc.u32 %1, t1, u1;\n\t"
-        "addc.u32 cm, z, z;\n\t"        // carry out
-        "neg.s32 cm, cm;\n\t"           // carry: + (2^32 - 1); cannot wrap again
-        "add.cc.u32 %0, %0, cm;\n\t"
-        "addc.u32 %1, %1, z;\n\t"
+        ".reg .u32 c, e0, e1;\n\t"
+        "mad.lo.cc.u32 %0, %4, 0xFFFFFFFF, %2;\n\t"
+        "madc.hi.cc.u32 %1, %4, 0xFFFFFFFF, %3;\n\t"
+        "addc.u32 c, 0, 0;\n\t"
+        "sub.cc.u32 %0, %0, %5;\n\t"
+        "subc.cc.u32 %1, %1, 0;\n\t"
+        "subc.u32 c, c, 0;\n\t"
+        "neg.s32 e0, c;\n\t"             // c*(2^32 - 1) as a signed 64-bit (e1:e0):
+        "shr.s32 e1, c, 31;\n\t"         // (0, 2^32 - 1), (0, 0) or (2^32 - 1, 1)
+        "add.cc.u32 %0, %0, e0;\n\t"
+        "addc.u32 %1, %1, e1;\n\t"
         "}"
         : "=r"(x0), "=r"(x1)
         : "r"(r0), "r"(r1), "r"(r2), "r"(r3));
     return ((uint64_t)x1 << 32) | x0;
-}
-
-// Canonical form of (r3:r2:r1:r0) mod p.  With t = (r1:r0) - r3 (+p on a
-// borrow) and u = r2*(2^32-1), x = t + u is below 2^65 - 2^33: if it carries,
-// x - 2^64 + (2^32 - 1) is already canonical (and does not carry); if not, x is
-// canonical unless x + (2^32 - 1) carries.  So one "add 2^32 - 1, keep it on
-// any carry" step both folds the carry and canonicalises.
-__device__ __forceinline__ uint64_t gl_reduce_limbs_c(uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3) {
-    uint32_t y0, y1;
-    asm("{\n\t"
-        ".reg .u32 t0, t1, bm, u0, u1, x0, x1, z0, z1, c;\n\t"
-        ".reg .pred q;\n\t"
-        "sub.cc.u32 t0, %2, %5;\n\t"    // t = (r1:r0) - r3
-        "subc.cc.u32 t1, %3, 0;\n\t"
-        "subc.u32 bm, 0, 0;\n\t"        // borrow mask
-        "sub.cc.u32 t0, t0, bm;\n\t"    // borrow: t -= 2^32 - 1 (i.e. + p)
-        "subc.u32 t1, t1, 0;\n\t"
-        "sub.cc.u32 u0, 0, %4;\n\t"     // u = (r2 << 32) - r2
-        "subc.u32 u1, %4, 0;\n\t"
-        "add.cc.u32 x0, t0, u0;\n\t"    // x = t + u, carry c
-        "addc.cc.u32 x1, t1, u1;\n\t"
-        "addc.u32 c, 0, 0;\n\t"
-        "add.cc.u32 z0, x0, 0xFFFFFFFF;\n\t"
-        "addc.cc.u32 z1, x1, 0;\n\t"
-        "addc.u32 c, c, 0;\n\t"
-        "setp.ne.u32 q, c, 0;\n\t"
-        "selp.b32 %0, z0, x0, q;\n\t"
-        "selp.b32 %1, z1, x1, q;\n\t"
-        "}"
-        : "=r"(y0), "=r"(y1)
-        : "r"(r0), "r"(r1), "r"(r2), "r"(r3));
-    return ((uint64_t)y1 << 32) | y0;
 }
 
 // a * b for any 64-bit representatives; partial result.
@@ -121,11 +90,7 @@ __device__ __forceinline__ uint64_t gl_mul(uint64_t a, uint64_t b) {
     return gl_reduce_limbs(r0, r1, r2, r3);
 }
 // a * b, canonical.
-__device__ __forceinline__ uint64_t gl_mul_c(uint64_t a, uint64_t b) {
-    uint32_t r0, r1, r2, r3;
-    gl_mul128(a, b, r0, r1, r2, r3);
-    return gl_reduce_limbs_c(r0, r1, r2, r3);
-}
+__device__ __forceinline__ uint64_t gl_mul_c(uint64_t a, uint64_t b) { return gl_canon(gl_mul(a, b)); }
 
 __device__ __forceinline__ uint64_t gl_sqr(uint64_t a) { return gl_mul(a, a); }
 
