@@ -332,6 +332,13 @@ int tvmc_server_create(const tvmc_server_config* cfg, tvmc_server** out);
  * TVMC_TRACE_DEVICE, TVMC_TRACE_ROW_MAJOR and TVMC_FRUGAL). */
 int tvmc_server_submit(tvmc_server* s, const uint64_t* trace, size_t trace_len, size_t width, uint32_t expansion,
                        uint64_t offset, uint32_t flags, uint64_t* request_id);
+/* Queue one randomized commitment (the arguments of tvmc_commit_randomized;
+ * flags may also hold TVMC_RAND_TRUNCATE).  The randomizer buffer, like the
+ * trace, must stay valid until tvmc_server_wait has returned. */
+int tvmc_server_submit_randomized(tvmc_server* s, const uint64_t* trace, size_t trace_len, size_t width,
+                                  uint32_t expansion, uint64_t trace_offset, uint64_t offset,
+                                  const uint64_t* randomizers, size_t num_randomizers, uint32_t flags,
+                                  uint64_t* request_id);
 /* Wait until the request is committed (timeout_ms < 0: no limit; expiry returns
  * TVMC_ERR_TIMEOUT) and copy its root; a request whose footprint exceeds the
  * whole budget fails with TVMC_ERR_NOMEM. */

@@ -115,3 +115,24 @@ def test_server_wait_timeout_and_times(tv):
         assert 0 < sub <= start <= done
         with pytest.raises(tv.InvalidArgument):
             srv.wait(rid + 1000)
+
+
+def test_server_randomized_requests(tv, oracle):
+    """Randomized (zero-knowledge) requests mixed with plain ones: each equals
+    tvmc_commit_randomized alone (and the oracle's tree for a small one)."""
+    specs = [(1 << 6, 23, 98, 3), (1 << 10, 64, 7, 1), (1 << 12, 379, 98, 5), (1 << 8, 10, 0, 1)]
+    tables = [(rand_u64(70 + i, (w, n)), rand_u64(80 + i, (w, R)), t) for i, (n, w, R, t) in enumerate(specs)]
+    with tv.Server(streams=3) as srv:
+        ids = [srv.submit(tr, randomizers=rnd, trace_offset=t) for tr, rnd, t in tables]
+        plain = srv.submit(tables[1][0])
+        for rid, (tr, rnd, t) in zip(ids, tables):
+            with tv.Commitment(tr, randomizers=rnd, trace_offset=t) as alone:
+                assert (srv.wait(rid) == alone.root()).all()
+                idx = [0, 3, 4 * tr.shape[1] - 1]
+                assert (srv.open(rid, idx) == alone.auth_paths(idx)).all()
+        with tv.Commitment(tables[1][0]) as alone:
+            assert (srv.wait(plain) == alone.root()).all()
+    tr, rnd, t = tables[0]
+    exp = oracle.merkle(oracle.hash_rows_cm(oracle.lde_randomized(tr, rnd, 4, 7, t)))
+    with tv.Commitment(tr, randomizers=rnd, trace_offset=t) as alone:
+        assert (alone.root() == exp[1]).all()

@@ -48,7 +48,9 @@ struct Request {
     const uint64_t* trace = nullptr;
     size_t n = 0, width = 0;
     uint32_t expansion = 4, flags = 0;
-    uint64_t offset = 7;
+    uint64_t offset = 7, trace_offset = 1;
+    const uint64_t* randomizers = nullptr;  // width x R, same side of the bus as the trace
+    size_t R = 0;
     size_t resident = 0, transient = 0;  // budget bytes held until release / until done
     bool large = false;
     int stream = -1;
@@ -72,8 +74,11 @@ void footprint(Request* r, bool keep_lde, size_t scratch_budget) {
     if (frugal) upload = (dev ? 0 : NW) + (rm ? NW : 0) + 6 * L * 8;
     else if (!dev && !rm) upload = 2 * std::min<size_t>(NW, size_t(256) << 20);
     else upload = (dev ? 0 : NW) + (rm ? NW : 0);
+    // randomized LDE: randomizer upload and the per-coset addends
+    const size_t rrows = r->R < N ? r->R : N;
+    const size_t rand = r->R ? (dev ? 0 : W * r->R * 8) + W * r->expansion * rrows * 8 : 0;
     r->resident = tree + (keep_lde && !frugal ? lde : 0);
-    r->transient = (keep_lde && !frugal ? 0 : lde) + scratch + upload;
+    r->transient = (keep_lde && !frugal ? 0 : lde) + scratch + upload + rand;
     r->large = L * std::max<size_t>(W, 1) * 8 > (size_t(128) << 20);
 }
 
@@ -169,12 +174,14 @@ void dispatch_loop(tvmc_server* s) {
         if (r->large) s->large_running++;
         r->state = State::Running;
         r->t_start = now_ns();
-        const uint32_t flags = (r->flags & (TVMC_TRACE_DEVICE | TVMC_TRACE_ROW_MAJOR | TVMC_FRUGAL)) |
+        const uint32_t flags = (r->flags & (TVMC_TRACE_DEVICE | TVMC_TRACE_ROW_MAJOR | TVMC_FRUGAL |
+                                            TVMC_RAND_TRUNCATE)) |
                                (s->keep_lde ? 0u : (uint32_t)TVMC_DISCARD_LDE);
         cudaStream_t st = s->streams[best];
         lk.unlock();
         tvmc_commitment* c = nullptr;
-        const int rc = tvmc_commit(r->trace, r->n, r->width, r->expansion, r->offset, flags, st, &c);
+        const int rc = tvmc_commit_randomized(r->trace, r->n, r->width, r->expansion, r->trace_offset, r->offset,
+                                              r->randomizers, r->R, flags, st, &c);
         const std::string err = rc ? tvmc_last_error() : "";
         lk.lock();
         auto undo = [&] {
@@ -254,9 +261,19 @@ int tvmc_server_create(const tvmc_server_config* cfg, tvmc_server** out) {
 
 int tvmc_server_submit(tvmc_server* s, const uint64_t* trace, size_t trace_len, size_t width, uint32_t expansion,
                        uint64_t offset, uint32_t flags, uint64_t* id) {
+    return tvmc_server_submit_randomized(s, trace, trace_len, width, expansion, 1, offset, nullptr, 0, flags, id);
+}
+
+int tvmc_server_submit_randomized(tvmc_server* s, const uint64_t* trace, size_t trace_len, size_t width,
+                                  uint32_t expansion, uint64_t trace_offset, uint64_t offset,
+                                  const uint64_t* randomizers, size_t num_randomizers, uint32_t flags,
+                                  uint64_t* id) {
     if (!s || !id) return tvmc::set_error(TVMC_ERR_INVALID, "null argument");
-    if (flags & ~(uint32_t)(TVMC_TRACE_DEVICE | TVMC_TRACE_ROW_MAJOR | TVMC_FRUGAL))
-        return tvmc::set_error(TVMC_ERR_INVALID, "server requests take only trace-layout and frugal flags");
+    if (flags & ~(uint32_t)(TVMC_TRACE_DEVICE | TVMC_TRACE_ROW_MAJOR | TVMC_FRUGAL | TVMC_RAND_TRUNCATE))
+        return tvmc::set_error(TVMC_ERR_INVALID, "server requests take only trace-layout, frugal and randomizer flags");
+    if (trace_offset % 0xFFFFFFFF00000001ull == 0)
+        return tvmc::set_error(TVMC_ERR_INVALID, "trace offset must be nonzero mod p");
+    if (width && num_randomizers && !randomizers) return tvmc::set_error(TVMC_ERR_INVALID, "null randomizers");
     if (!trace_len || (trace_len & (trace_len - 1)) || trace_len > (size_t(1) << TVMC_MAX_LOG_LDE_TRACE))
         return tvmc::set_error(TVMC_ERR_INVALID, "trace length is not a supported power of 2");
     if (!expansion || (expansion & (expansion - 1)) || expansion > 16)
@@ -268,6 +285,9 @@ int tvmc_server_submit(tvmc_server* s, const uint64_t* trace, size_t trace_len, 
     r->width = width;
     r->expansion = expansion;
     r->offset = offset;
+    r->trace_offset = trace_offset;
+    r->randomizers = randomizers;
+    r->R = width ? num_randomizers : 0;
     r->flags = flags;
     r->t_submit = now_ns();
     std::lock_guard<std::mutex> lk(s->mu);

@@ -122,6 +122,9 @@ SIGNATURES = {
     "tvmc_server_create": (ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),
     "tvmc_server_submit": (ctypes.c_int, [_vp, _vp, _sz, _sz, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint32,
                                           ctypes.POINTER(ctypes.c_uint64)]),
+    "tvmc_server_submit_randomized": (ctypes.c_int, [_vp, _vp, _sz, _sz, ctypes.c_uint32, ctypes.c_uint64,
+                                                     ctypes.c_uint64, _vp, _sz, ctypes.c_uint32,
+                                                     ctypes.POINTER(ctypes.c_uint64)]),
     "tvmc_server_wait": (ctypes.c_int, [_vp, ctypes.c_uint64, ctypes.c_int64, _u64p]),
     "tvmc_server_open": (ctypes.c_int, [_vp, ctypes.c_uint64, _szp, _sz, _u64p, _u64p]),
     "tvmc_server_times": (ctypes.c_int, [_vp, ctypes.c_uint64, _u64p, _u64p, _u64p]),
@@ -594,8 +597,11 @@ class Server:
         self._meta = {}  # id -> (height, width, trace buffer kept alive until committed)
 
     def submit(self, trace, expansion: int = 4, offset: int = 7, row_major: bool = False, frugal: bool = False,
-               width: int | None = None, trace_len: int | None = None, device_ptr: bool = False) -> int:
-        flags = (TRACE_ROW_MAJOR if row_major else 0) | (FRUGAL if frugal else 0)
+               width: int | None = None, trace_len: int | None = None, device_ptr: bool = False,
+               randomizers=None, trace_offset: int = 1, truncate: bool = False) -> int:
+        """randomizers: host (width, R) array, or with device_ptr=True (pointer, R)."""
+        flags = (TRACE_ROW_MAJOR if row_major else 0) | (FRUGAL if frugal else 0) | \
+            (RAND_TRUNCATE if truncate else 0)
         if device_ptr:
             flags |= TRACE_DEVICE
             ptr, keep = int(trace), None
@@ -603,8 +609,17 @@ class Server:
             t = _u64(trace)
             trace_len, width = t.shape if row_major else t.shape[::-1]
             ptr, keep = (t.ctypes.data if t.size else None), t
+        rptr, R = None, 0
+        if randomizers is not None:
+            if device_ptr:
+                rptr, R = int(randomizers[0]), int(randomizers[1])
+            else:
+                r = _u64(randomizers).reshape(width, -1)
+                rptr, R = (r.ctypes.data if r.size else None), r.shape[1]
+                keep = (keep, r)
         rid = ctypes.c_uint64(0)
-        _check(lib().tvmc_server_submit(self.h, ptr, trace_len, width, expansion, offset, flags, ctypes.byref(rid)))
+        _check(lib().tvmc_server_submit_randomized(self.h, ptr, trace_len, width, expansion, trace_offset, offset,
+                                                   rptr, R, flags, ctypes.byref(rid)))
         self._meta[rid.value] = ((trace_len * expansion).bit_length() - 1, width, keep)
         return rid.value
 
