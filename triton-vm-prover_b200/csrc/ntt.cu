@@ -328,8 +328,12 @@ __global__ void __launch_bounds__(NTT_THREADS) k_lde_small(const uint64_t* trace
 }
 
 // K1: inverse pass A over the trace: Y[i1 + n1*k2] = w^-(i1*k2) DFT^-1_n2(...)[k2].
+// At 2^10-point passes the unbounded allocation takes 136 registers (one
+// 256-thread CTA per SM); capping it at two CTAs per SM is 4% faster on the
+// 2^20-row LDE.  The other kernels keep their unbounded allocations, which
+// measured faster than capped ones.
 template <int L2>
-__global__ void __launch_bounds__(NTT_THREADS) k_lde_inv_a(const uint64_t* trace, uint64_t tld, uint64_t* Y,
+__global__ void __launch_bounds__(NTT_THREADS, L2 == 10 ? 2 : 1) k_lde_inv_a(const uint64_t* trace, uint64_t tld, uint64_t* Y,
                                                            uint64_t yld, int l1, int lT, const uint64_t* tw12_i,
                                                            const uint64_t* wlo, const uint64_t* whi) {
     extern __shared__ uint64_t sm[];
