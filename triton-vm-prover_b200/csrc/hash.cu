@@ -17,6 +17,8 @@ namespace tvmc {
 
 constexpr int HASH_THREADS = 256;
 constexpr int UP_THREADS = 128;
+// Tree levels with at least this many parents are built one level per launch.
+constexpr uint64_t MERKLE_LEVEL_MIN_PARENTS = 1ull << 16;
 
 __device__ __forceinline__ void store_digest(uint64_t* p, const uint64_t d[5]) {
 #pragma unroll
@@ -169,6 +171,25 @@ __global__ void __launch_bounds__(UP_THREADS) k_merkle_up(uint64_t* __restrict__
     }
 }
 
+// One tree level: parent p in [m/2, m) = hash_pair(node 2p, node 2p + 1), one
+// parent per thread.  Used while a level has enough parents to fill the GPU;
+// adjacent parents read adjacent child pairs, so loads and stores coalesce.
+__global__ void __launch_bounds__(HASH_THREADS) k_merkle_level(uint64_t* __restrict__ tree, uint64_t n, uint64_t m,
+                                                               int layout) {
+    __shared__ uint32_t sbox[T5_SBOX_WORDS];
+    t5_sbox_init(sbox);
+    __syncthreads();
+    const uint64_t par = (m >> 1) + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (par >= m) return;
+    const uint64_t* l = tree + 5 * node_slot(2 * par, n, layout);
+    const uint64_t* r = tree + 5 * node_slot(2 * par + 1, n, layout);
+    uint64_t a[5], b[5], h[5];
+#pragma unroll
+    for (int i = 0; i < 5; i++) { a[i] = l[i]; b[i] = r[i]; }
+    t5_hash_pair(a, b, h, sbox + (threadIdx.x & 31));
+    store_digest(tree + 5 * node_slot(par, n, layout), h);
+}
+
 __global__ void k_copy_leaves(const uint64_t* __restrict__ leaves, uint64_t* __restrict__ tree, uint64_t n,
                               int layout) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -295,13 +316,21 @@ static inline unsigned grid_for(uint64_t work, unsigned threads) {
     return (unsigned)((work + threads - 1) / threads);
 }
 
-cudaError_t launch_merkle_from_leaves(uint64_t* tree, uint64_t n, int layout, cudaStream_t st) {
-    // n leaves already in place; build all levels above.
-    uint64_t m = n;
+// The m nodes of one level (heap indices [m, 2m)) of a tree with n leaves are
+// in place: build every level above.  Wide levels go one per launch with every
+// thread busy; the rest, 8 levels per launch in shared memory.
+static cudaError_t launch_tree_above(uint64_t* tree, uint64_t n, uint64_t m, int layout, cudaStream_t st) {
+    while ((m >> 1) >= MERKLE_LEVEL_MIN_PARENTS) {
+        count_launch();
+        k_merkle_level<<<grid_for(m >> 1, HASH_THREADS), HASH_THREADS, 0, st>>>(tree, n, m, layout);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        m >>= 1;
+    }
     while (m > 1) {
-        uint64_t parents = m >> 1;
-        unsigned threads = (unsigned)(parents < UP_THREADS ? parents : UP_THREADS);
-        int levels = ilog2u(threads) + 1;
+        const uint64_t parents = m >> 1;
+        const unsigned threads = (unsigned)(parents < UP_THREADS ? parents : UP_THREADS);
+        const int levels = ilog2u(threads) + 1;
         count_launch();
         k_merkle_up<<<grid_for(parents, threads), threads, 0, st>>>(tree, n, m, layout, levels);
         cudaError_t e = cudaGetLastError();
@@ -309,6 +338,10 @@ cudaError_t launch_merkle_from_leaves(uint64_t* tree, uint64_t n, int layout, cu
         m >>= levels;
     }
     return cudaSuccess;
+}
+
+cudaError_t launch_merkle_from_leaves(uint64_t* tree, uint64_t n, int layout, cudaStream_t st) {
+    return launch_tree_above(tree, n, n, layout, st);  // n leaves already in place
 }
 
 cudaError_t launch_hash_rows(const uint64_t* table, uint64_t rstride, uint64_t cstride, uint64_t rows,
@@ -329,18 +362,7 @@ cudaError_t launch_hash_rows(const uint64_t* table, uint64_t rstride, uint64_t c
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     // the block subtrees are complete up to `fuse` levels; continue from there
-    uint64_t m = rows >> fuse;
-    while (m > 1) {
-        uint64_t parents = m >> 1;
-        unsigned th = (unsigned)(parents < UP_THREADS ? parents : UP_THREADS);
-        int levels = ilog2u(th) + 1;
-        count_launch();
-        k_merkle_up<<<grid_for(parents, th), th, 0, st>>>(tree, rows, m, layout, levels);
-        e = cudaGetLastError();
-        if (e != cudaSuccess) return e;
-        m >>= levels;
-    }
-    return cudaSuccess;
+    return launch_tree_above(tree, rows, rows >> fuse, layout, st);
 }
 
 cudaError_t launch_merkle_tree(const uint64_t* leaves, uint64_t* tree, uint64_t n, int layout,
@@ -416,17 +438,7 @@ cudaError_t launch_absorb_stripe(const uint64_t* stripe, uint64_t L, uint32_t nc
     k_absorb_stripe<<<(unsigned)(L / threads), threads, 0, st>>>(stripe, L, ncols, cap, first, last, tree, fuse);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess || !last) return e;
-    uint64_t m = L >> fuse;  // complete the tree above the block subtrees
-    while (m > 1) {
-        const uint64_t parents = m >> 1;
-        const unsigned th = (unsigned)(parents < UP_THREADS ? parents : UP_THREADS);
-        const int levels = 63 - __builtin_clzll(th) + 1;
-        count_launch();
-        k_merkle_up<<<(unsigned)(parents / th), th, 0, st>>>(tree, L, m, LAYOUT_HEAP, levels);
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        m >>= levels;
-    }
-    return cudaSuccess;
+    return launch_tree_above(tree, L, L >> fuse, LAYOUT_HEAP, st);  // complete the tree above the block subtrees
 }
 
 }  // namespace tvmc
