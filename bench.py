@@ -325,10 +325,10 @@ def run_ours(args):
         hbm_peak, hbm_src = float(json.load(open(peaks_path))["hbm_gbs"]), "measured"
     int_peak = int_peak_tops(torch, dev)
     # DRAM bytes per k_hash_rows launch: one ncu capture of the 2^18-row x 379-column
-    # main-table launch (796.1 MB read + 20.5 MB written), scaled by rows
+    # main-table launch (796.6 MB read + 12.2 MB written), scaled by rows
     traffic, traffic_src = None, None
     if W_MAIN == 379:
-        traffic = (796.1e6 + 20.5e6) * L / (1 << 18)
+        traffic = (796.6e6 + 12.2e6) * L / (1 << 18)
         traffic_src = "ncu dram__bytes_read+write of a 2^18x379 launch, scaled by LDE rows (main table)"
 
     # e2e: pinned host traces through the public C ABI, roots read back
@@ -646,7 +646,8 @@ def main():
     ap.add_argument("--requests", type=int, default=48, help="serving: requests per rate")
     ap.add_argument("--serve-streams", type=int, default=4)
     ap.add_argument("--serve-max-log-n", type=int, default=20)
-    ap.add_argument("--serve-max-large", type=int, default=1, help="serving: large tables committed at once")
+    ap.add_argument("--serve-max-large", type=int, default=0,
+                    help="serving: large tables issued at once (0: the server's default)")
     ap.add_argument("--serve-loads", type=float, nargs="+", default=[0.5, 0.9, 1.5, 3.0],
                     help="serving: offered load as a multiple of the plain path's capacity")
     args = ap.parse_args()

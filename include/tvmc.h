@@ -209,12 +209,17 @@ typedef struct tvmc_commitment tvmc_commitment;
  *                         eight inside the row-hash CTAs; default 0
  * Unknown keys return TVMC_ERR_INVALID. */
 int tvmc_set_tuning(const char* key, long long value);
-/* The library keeps its LDE/NTT scratch and upload staging per (device, stream)
- * once used, and the device's stream-ordered memory pool keeps freed memory, so
- * that repeated commits never wait for the driver to map memory.  This frees
+/* The library keeps its LDE/NTT scratch, upload staging and the LDE of
+ * TVMC_DISCARD_LDE commitments per (device, stream) once used, and the device's
+ * stream-ordered memory pool keeps freed memory, so that repeated commits never
+ * wait for the driver to map memory.  This frees
  * that scratch and returns the pool's unused memory on the current device; it
  * synchronizes the device first. */
 int tvmc_release_cached_memory(void);
+/* Frees the buffers this library keeps for one stream (and its upload stream),
+ * ordered after the work already queued on it.  Call before destroying a
+ * stream that was passed to this library, so that its memory is not held. */
+int tvmc_forget_stream(void* stream);
 int tvmc_get_tuning(const char* key, long long* value);
 
 /* Commit to one table: LDE of every column onto offset * <w_{trace_len*expansion}>
@@ -303,9 +308,9 @@ int tvmc_batch_free(tvmc_batch* b);
  * running requests and the trees still held, and is issued at once on the
  * least-loaded of its worker streams.  Small tables (LDE up to 128 MB) run
  * concurrently on num_streams high-priority streams and never wait behind
- * large ones; large tables, each enough to fill the GPU, run
- * max_large_inflight at a time in arrival order, each slot with its own
- * stream.  Each request's
+ * large ones; large tables, each enough to fill the GPU, go in arrival order
+ * onto one dedicated stream, with up to max_large_inflight of them issued at
+ * once (the next one's upload overlaps the current one's kernels).  Each request's
  * Merkle tree stays on the device for openings until tvmc_server_release;
  * with TVMC_SERVER_KEEP_LDE its LDE stays too (rows can be opened).  Results
  * are bit-identical to tvmc_commit of the same table alone.  The trace buffer
@@ -319,7 +324,7 @@ typedef struct tvmc_server_config {
     size_t hbm_budget_bytes; /* 0: 90% of the device memory free at creation */
     uint32_t num_streams;    /* worker streams for small tables, 0: 4 (at most 64) */
     uint32_t flags;          /* TVMC_SERVER_KEEP_LDE */
-    uint32_t max_large_inflight; /* large tables committed at once, 0: 1 (at most 16) */
+    uint32_t max_large_inflight; /* large tables issued at once, 0: 2 (at most 16) */
 } tvmc_server_config;
 
 typedef struct tvmc_server_stats {

@@ -129,3 +129,39 @@ def test_tuning_knobs_do_not_change_results(tv, oracle, knob, value, logn):
         tv.set_tuning(knob, 0)
     if logn == 4:
         assert (exp[1:] == oracle.merkle(oracle.hash_rows_cm(oracle.lde(t)))[1:]).all()
+
+
+def test_back_to_back_host_commits_share_staging_safely(tv):
+    """Host-trace commits issued back to back on one stream reuse its upload
+    staging buffers, the next upload overlapping the previous commit's row hash.
+    2^17 x 379 traces upload in several chunks; every root must equal the
+    device-input commit's (which uses no staging)."""
+    import torch
+    tables = [rand_u64(0x5EED00 + i, (379, 1 << 17)) for i in range(3)]
+    stream = torch.cuda.Stream()
+    commits = [tv.Commitment(t, stream=stream.cuda_stream, discard_lde=True) for t in tables]
+    roots = [c.root() for c in commits]
+    for c in commits:
+        c.free()
+    for t, r in zip(tables, roots):
+        d = torch.from_numpy(t.view(np.int64)).cuda()
+        with tv.Commitment(d.data_ptr(), width=t.shape[0], trace_len=t.shape[1], device_ptr=True) as ref:
+            assert (r == ref.root()).all()
+    torch.cuda.synchronize()
+
+
+def test_forget_stream_then_reuse(tv):
+    """tvmc_forget_stream frees a stream's cached buffers; later commits on the
+    same stream (or a new one) rebuild them and give the same root."""
+    import torch
+    t = rand_u64(0x0F0F, (64, 1 << 12))
+    s = torch.cuda.Stream()
+    with tv.Commitment(t, stream=s.cuda_stream, discard_lde=True) as a:
+        ra = a.root()
+    tv.forget_stream(s.cuda_stream)
+    with tv.Commitment(t, stream=s.cuda_stream, discard_lde=True) as b:
+        assert (b.root() == ra).all()
+    tv.forget_stream(s.cuda_stream)
+    tv.release_cached_memory()
+    with tv.Commitment(t) as c:
+        assert (c.root() == ra).all()

@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <tuple>
@@ -250,12 +251,19 @@ uint64_t plan_offset(uint64_t t, uint64_t o) { return hmul(o % P, hinv(t % P)); 
 struct ScratchSlot {
     uint64_t* p = nullptr;
     size_t words = 0;
+    // staging slots: completes when the last kernel reading the buffer is done
+    // (the next upload into it waits for this, not for the whole stream)
+    cudaEvent_t last_use = nullptr;
 };
-// kind: 0 = LDE/NTT intermediates, 1 and 2 = the two upload staging buffers.
+// kind: 0 = LDE/NTT intermediates, 1 and 2 = the two upload staging buffers,
+// 3 = the LDE of commits that discard it after hashing.
 std::map<std::tuple<int, cudaStream_t, int>, ScratchSlot> g_scratch;  // guarded by g_mu
 
-int stream_scratch(cudaStream_t st, size_t words, uint64_t** out, int kind = 0) {
+// *grown (optional) is set when the buffer was (re)allocated by this call, i.e.
+// it becomes usable only in stream order on st.
+int stream_scratch(cudaStream_t st, size_t words, uint64_t** out, int kind = 0, bool* grown = nullptr) {
     *out = nullptr;
+    if (grown) *grown = false;
     if (words == 0) return TVMC_OK;
     int dev;
     CK(cudaGetDevice(&dev));
@@ -263,12 +271,53 @@ int stream_scratch(cudaStream_t st, size_t words, uint64_t** out, int kind = 0) 
     ScratchSlot& slot = g_scratch[{dev, st, kind}];
     if (slot.words < words) {
         if (slot.p) cudaFreeAsync(slot.p, st);  // ordered after the work that used it
+        if (slot.last_use) cudaEventDestroy(slot.last_use);
         slot = ScratchSlot{};
         CK(cudaMallocAsync((void**)&slot.p, words * 8, st));
         slot.words = words;
+        if (grown) *grown = true;
     }
     *out = slot.p;
     return TVMC_OK;
+}
+
+// Commits enqueueing uploads on one stream take turns (the staging buffers and
+// their last-use events are per stream); other streams are not held up.
+std::map<std::pair<int, cudaStream_t>, std::unique_ptr<std::mutex>> g_upload_mu;  // guarded by g_mu
+
+std::mutex& upload_mutex(cudaStream_t st) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto& m = g_upload_mu[{dev, st}];
+    if (!m) m = std::make_unique<std::mutex>();
+    return *m;
+}
+
+// The last-use event of a staging slot: take it (the caller now owns it, or
+// gets null) or hand a new one over (the slot then owns it).
+cudaEvent_t take_slot_event(cudaStream_t st, int kind) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto it = g_scratch.find({dev, st, kind});
+    if (it == g_scratch.end()) return nullptr;
+    cudaEvent_t ev = it->second.last_use;
+    it->second.last_use = nullptr;
+    return ev;
+}
+
+void give_slot_event(cudaStream_t st, int kind, cudaEvent_t ev) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto it = g_scratch.find({dev, st, kind});
+    if (it == g_scratch.end()) {
+        cudaEventDestroy(ev);
+        return;
+    }
+    if (it->second.last_use) cudaEventDestroy(it->second.last_use);
+    it->second.last_use = ev;
 }
 
 int run_lde(const LdePlan& pl, const uint64_t* d_tr, uint64_t tld, uint64_t* d_out, uint64_t old, size_t width,
@@ -321,20 +370,28 @@ int upload_lde_pipelined(const LdePlan& pl, const uint64_t* h_trace, size_t n, s
     size_t stage_cols = std::max<size_t>(1, (size_t(256) << 20) / (n * 8));
     chunk = std::min(chunk, stage_cols);
     const size_t nchunks = (width + chunk - 1) / chunk;
+    std::lock_guard<std::mutex> turn(upload_mutex(st));
     uint64_t *scratch = nullptr, *stage[2] = {nullptr, nullptr};
-    cudaEvent_t ready[2] = {nullptr, nullptr}, freed[2] = {nullptr, nullptr};
+    cudaEvent_t ready[2] = {nullptr, nullptr}, freed[2] = {nullptr, nullptr}, prev[2] = {nullptr, nullptr};
+    bool used[2] = {false, false};
     if ((rc = stream_scratch(st, lde_scratch_words(pl.logn, pl.log_exp, chunk), &scratch))) return rc;
     cudaError_t e = cudaSuccess;
     for (int b = 0; b < 2 && e == cudaSuccess; b++) {
-        if (stream_scratch(st, chunk * n, &stage[b], 1 + b)) e = cudaErrorMemoryAllocation;
+        bool grown = false;
+        if (stream_scratch(st, chunk * n, &stage[b], 1 + b, &grown)) e = cudaErrorMemoryAllocation;
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ready[b], cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&freed[b], cudaEventDisableTiming);
-        if (e == cudaSuccess) e = cudaEventRecord(freed[b], st);  // allocations are ordered on st
+        // The first copy into stage[b] waits for the last kernel that read it (the
+        // previous commit's on this stream), so it can overlap that commit's row
+        // hash; a freshly allocated buffer is ordered on st instead.
+        if (e == cudaSuccess && !grown) prev[b] = take_slot_event(st, 1 + b);
+        if (e == cudaSuccess && !prev[b]) e = cudaEventRecord(freed[b], st);
     }
     for (size_t k = 0; k < nchunks && e == cudaSuccess; k++) {
         const int b = (int)(k & 1);
         const size_t c0 = k * chunk, nc = std::min(chunk, width - c0);
-        e = cudaStreamWaitEvent(cs, freed[b], 0);
+        e = cudaStreamWaitEvent(cs, (!used[b] && prev[b]) ? prev[b] : freed[b], 0);
+        used[b] = true;
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(stage[b], h_trace + c0 * n, nc * n * 8, cudaMemcpyHostToDevice, cs);
         if (e == cudaSuccess) e = cudaEventRecord(ready[b], cs);
@@ -344,7 +401,13 @@ int upload_lde_pipelined(const LdePlan& pl, const uint64_t* h_trace, size_t n, s
     }
     for (int b = 0; b < 2; b++) {
         if (ready[b]) cudaEventDestroy(ready[b]);  // destruction is deferred until the event completes
-        if (freed[b]) cudaEventDestroy(freed[b]);
+        if (e == cudaSuccess && used[b]) {
+            give_slot_event(st, 1 + b, freed[b]);  // recorded after the last kernel reading stage[b]
+            if (prev[b]) cudaEventDestroy(prev[b]);
+        } else {
+            if (freed[b]) cudaEventDestroy(freed[b]);
+            if (prev[b]) give_slot_event(st, 1 + b, prev[b]);  // still the guard for that buffer
+        }
     }
     if (e != cudaSuccess) return cuda_fail(e, "pipelined upload/LDE");
     return TVMC_OK;
@@ -537,13 +600,14 @@ struct tvmc_commitment {
     cudaEvent_t prof[4] = {nullptr, nullptr, nullptr, nullptr};
     bool batch_owned = false;  // freed by tvmc_batch_free only
     bool pooled = false;       // buffers from cudaMallocAsync on `stream`
+    bool lde_borrowed = false; // d_lde is the stream's cached buffer (TVMC_DISCARD_LDE), not owned
 };
 
 namespace {
 void destroy_commitment(tvmc_commitment* c) {
     if (c->pooled) {
         // ordered after the commitment's own work on its stream; the host does not wait
-        if (c->d_lde) cudaFreeAsync(c->d_lde, c->stream);
+        if (c->d_lde && !c->lde_borrowed) cudaFreeAsync(c->d_lde, c->stream);
         if (c->d_nodes) cudaFreeAsync(c->d_nodes, c->stream);
         if (c->done) cudaEventDestroy(c->done);
     } else {
@@ -637,6 +701,36 @@ int tvmc_version(void) { return 1; }
 
 unsigned long long tvmc_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
+int tvmc_forget_stream(void* stream) {
+    cudaStream_t st = as_stream(stream);
+    int dev;
+    CK(cudaGetDevice(&dev));
+    cudaStream_t cs = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        for (auto it = g_scratch.begin(); it != g_scratch.end();) {
+            if (std::get<0>(it->first) == dev && std::get<1>(it->first) == st) {
+                if (it->second.p) cudaFreeAsync(it->second.p, st);  // after the stream's queued work
+                if (it->second.last_use) cudaEventDestroy(it->second.last_use);
+                it = g_scratch.erase(it);
+            } else {
+                ++it;
+            }
+        }
+        auto c = g_copy_streams.find({dev, st});
+        if (c != g_copy_streams.end()) {
+            cs = c->second;
+            g_copy_streams.erase(c);
+        }
+        g_upload_mu.erase({dev, st});
+    }
+    if (cs) {
+        CK(cudaStreamSynchronize(cs));
+        CK(cudaStreamDestroy(cs));
+    }
+    return TVMC_OK;
+}
+
 int tvmc_release_cached_memory(void) {
     int dev;
     CK(cudaGetDevice(&dev));
@@ -646,6 +740,7 @@ int tvmc_release_cached_memory(void) {
         for (auto it = g_scratch.begin(); it != g_scratch.end();) {
             if (std::get<0>(it->first) == dev) {
                 if (it->second.p) cudaFree(it->second.p);
+                if (it->second.last_use) cudaEventDestroy(it->second.last_use);
                 it = g_scratch.erase(it);
             } else {
                 ++it;
@@ -1002,9 +1097,18 @@ int tvmc_commit_randomized(const uint64_t* trace, size_t trace_len, size_t width
     // stream-ordered pool memory: repeated commits reuse it without page mapping,
     // and freeing a commitment never stalls the device
     c->pooled = true;
+    // An LDE that is discarded after hashing lives in the stream's cached buffer
+    // (kind 3), so a run of commits of varying sizes does not fragment the pool
+    // with multi-GB blocks (a later, larger one would then grow the pool, and the
+    // host would stall while the driver maps memory).  Work on the stream runs in
+    // order, so the next commit reuses it only after this one's hash.
+    c->lde_borrowed = width && !frugal && (flags & TVMC_DISCARD_LDE);
     if (cudaMallocAsync((void**)&c->d_nodes, 2 * c->L * 40, st) != cudaSuccess ||
-        (width && !frugal && cudaMallocAsync((void**)&c->d_lde, c->L * width * 8, st) != cudaSuccess)) {
+        (width && !frugal &&
+         (c->lde_borrowed ? stream_scratch(st, c->L * width, &c->d_lde, 3) != TVMC_OK
+                          : cudaMallocAsync((void**)&c->d_lde, c->L * width * 8, st) != cudaSuccess))) {
         cudaGetLastError();
+        if (c->lde_borrowed) c->d_lde = nullptr;
         return bail(fail(TVMC_ERR_NOMEM, "cannot allocate LDE (%zu x %zu) and tree", c->L, width));
     }
     if (cudaMemsetAsync(c->d_nodes, 0, 40, st) != cudaSuccess) return bail(cuda_fail(cudaGetLastError(), "memset"));
@@ -1090,7 +1194,7 @@ int tvmc_commit_randomized(const uint64_t* trace, size_t trace_len, size_t width
     }
     if (prof) cudaEventRecord(c->prof[3], st);
     if ((flags & TVMC_DISCARD_LDE) && c->d_lde) {
-        cudaFreeAsync(c->d_lde, st);  // stream-ordered after the hash kernel
+        if (!c->lde_borrowed) cudaFreeAsync(c->d_lde, st);  // stream-ordered after the hash kernel
         c->d_lde = nullptr;
     }
     if (cudaEventCreateWithFlags(&c->done, cudaEventDisableTiming) != cudaSuccess ||

@@ -6,11 +6,13 @@
 // dispatcher admits a queue head as soon as its device footprint fits the HBM
 // budget next to what running requests and resident trees already hold --
 // small tables at once, on high-priority worker streams, and large tables up
-// to a limit in flight (default 1: two GPU-filling commits only share the
-// GPU), each on its own dedicated stream, so that the stream-ordered memory
-// pool hands a large commit's multi-GB buffers straight to the next one --
-// so small requests never wait behind large ones and requests of mixed sizes
-// overlap as they arrive.  A host callback
+// to a limit in flight (default 2) on one dedicated stream: two GPU-filling
+// commits running side by side were measured slower than one after the other,
+// but a second one issued behind the first gets its uploads and launches
+// queued while the first computes, and the stream's cached LDE, scratch and
+// staging buffers pass from one large commit to the next -- so small requests
+// never wait behind large ones and requests of mixed sizes overlap as they
+// arrive.  A host callback
 // on the stream marks each request done, records its completion time and
 // returns its transient memory to the budget; its Merkle tree (and, with
 // TVMC_SERVER_KEEP_LDE, its LDE) stays on the device for openings until the
@@ -235,12 +237,12 @@ int tvmc_server_create(const tvmc_server_config* cfg, tvmc_server** out) {
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return tvmc::set_error(TVMC_ERR_CUDA, "cudaMemGetInfo");
     s->budget = c.hbm_budget_bytes ? c.hbm_budget_bytes : free_b / 10 * 9;
     s->keep_lde = c.flags & TVMC_SERVER_KEEP_LDE;
-    s->max_large = c.max_large_inflight ? (int)c.max_large_inflight : 1;
+    s->max_large = c.max_large_inflight ? (int)c.max_large_inflight : 2;
     long long sb = 0;
     if (tvmc_get_tuning("lde_scratch_bytes", &sb) == TVMC_OK && sb > 0) s->scratch_budget = (size_t)sb;
     s->n_small = c.num_streams ? (int)std::min<uint32_t>(c.num_streams, 64) : 4;
     s->max_large = (int)std::min<uint32_t>(s->max_large, 16);
-    const int ns = s->n_small + s->max_large;
+    const int ns = s->n_small + 1;  // small-table streams + the large-table stream
     int lo_prio = 0, hi_prio = 0;
     cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio);
     for (int i = 0; i < ns; i++) {
@@ -392,7 +394,10 @@ int tvmc_server_destroy(tvmc_server* s) {
     for (auto st : s->streams) cudaStreamSynchronize(st);  // every on_done has run
     for (auto& kv : s->reqs)
         if (kv.second->c) tvmc_commitment_free(kv.second->c);
-    for (auto st : s->streams) cudaStreamDestroy(st);
+    for (auto st : s->streams) {
+        tvmc_forget_stream(st);  // the library's cached buffers for this stream
+        cudaStreamDestroy(st);
+    }
     delete s;
     return TVMC_OK;
 }

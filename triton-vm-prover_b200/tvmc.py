@@ -119,6 +119,7 @@ SIGNATURES = {
     "tvmc_batch_commitment": (ctypes.c_int, [_vp, _sz, ctypes.POINTER(_vp)]),
     "tvmc_batch_free": (ctypes.c_int, [_vp]),
     "tvmc_release_cached_memory": (ctypes.c_int, []),
+    "tvmc_forget_stream": (ctypes.c_int, [_vp]),
     "tvmc_server_create": (ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),
     "tvmc_server_submit": (ctypes.c_int, [_vp, _vp, _sz, _sz, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint32,
                                           ctypes.POINTER(ctypes.c_uint64)]),
@@ -286,6 +287,11 @@ def set_tuning(key: str, value: int) -> None:
 def release_cached_memory() -> None:
     """Free the per-stream scratch and trim the device pool (synchronizes)."""
     _check(lib().tvmc_release_cached_memory())
+
+
+def forget_stream(stream) -> None:
+    """Free the library's cached buffers for a stream about to be destroyed."""
+    _check(lib().tvmc_forget_stream(_stream(stream)))
 
 
 def get_tuning(key: str) -> int:
