@@ -241,6 +241,25 @@ int tvmc_commit(const uint64_t* trace, size_t trace_len, size_t width, uint32_t 
 int tvmc_commit_randomized(const uint64_t* trace, size_t trace_len, size_t width, uint32_t expansion,
                            uint64_t trace_offset, uint64_t offset, const uint64_t* randomizers,
                            size_t num_randomizers, uint32_t flags, void* stream, tvmc_commitment** out);
+/* Commitment to rows that are already evaluated, with no LDE: the quotient
+ * segments' table (leaf = hash_xfield_row of each row, src/stark.cpp:759-764 and
+ * 1942-1987, TableCommitment::from_digests src/table/table_commitment.cpp) or any
+ * other codeword table.  Leaf r = Tip5 hash_varlen of row r; num_rows must be a
+ * power of two.  Flags: TVMC_TRACE_DEVICE, TVMC_TRACE_ROW_MAJOR (as for
+ * tvmc_commit), TVMC_DISCARD_LDE (keep only the tree; otherwise a column-major
+ * copy of the rows is kept for tvmc_commitment_read_rows), TVMC_SYNC.  The
+ * handle's "LDE" is the table itself (tvmc_commitment_shape: lde_len = num_rows). */
+int tvmc_commit_rows(const uint64_t* table, size_t num_rows, size_t width, uint32_t flags, void* stream,
+                     tvmc_commitment** out);
+
+#define TVMC_LEAVES_XFE 0x80u /* tvmc_commit_digests: leaves are XFieldElements (3 words each) */
+/* Commitment to given leaves: a Merkle tree over num_leaves digests (5 words
+ * each; MerkleTree(leaves), TableCommitment::from_digests), or with
+ * TVMC_LEAVES_XFE over an XFieldElement codeword whose element i becomes the leaf
+ * (c0, c1, c2, 0, 0) with no hashing -- the FRI round trees (src/fri/fri.cpp:25-43,
+ * 715-730).  Host leaves, or device leaves with TVMC_TRACE_DEVICE; TVMC_SYNC. */
+int tvmc_commit_digests(const uint64_t* leaves, size_t num_leaves, uint32_t flags, void* stream,
+                        tvmc_commitment** out);
 /* Wait for the commitment and copy its root (5 words) to host memory. */
 int tvmc_commitment_root(tvmc_commitment* c, uint64_t* root);
 int tvmc_commitment_sync(tvmc_commitment* c);

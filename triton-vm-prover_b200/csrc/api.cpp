@@ -1207,6 +1207,118 @@ int tvmc_commit_randomized(const uint64_t* trace, size_t trace_len, size_t width
     return TVMC_OK;
 }
 
+// Shared tail of the rows/digests commitments: completion event, optional sync.
+static int finish_commitment(tvmc_commitment* c, uint32_t flags, tvmc_commitment** out) {
+    if (cudaEventCreateWithFlags(&c->done, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventRecord(c->done, c->stream) != cudaSuccess) {
+        const int rc = cuda_fail(cudaGetLastError(), "event");
+        tvmc_commitment_free(c);
+        return rc;
+    }
+    if ((flags & TVMC_SYNC) && cudaEventSynchronize(c->done) != cudaSuccess) {
+        const int rc = cuda_fail(cudaGetLastError(), "sync");
+        tvmc_commitment_free(c);
+        return rc;
+    }
+    *out = c;
+    return TVMC_OK;
+}
+
+int tvmc_commit_rows(const uint64_t* table, size_t num_rows, size_t width, uint32_t flags, void* stream,
+                     tvmc_commitment** out) {
+    if (!out) return fail(TVMC_ERR_INVALID, "null output handle");
+    *out = nullptr;
+    if (flags & ~(TVMC_TRACE_DEVICE | TVMC_TRACE_ROW_MAJOR | TVMC_DISCARD_LDE | TVMC_SYNC))
+        return fail(TVMC_ERR_INVALID, "unknown flag bits 0x%x", flags);
+    if (!is_pow2(num_rows)) return fail(TVMC_ERR_INVALID, "Number of leaves must be a power of 2 (got %zu)", num_rows);
+    if (width && !table) return fail(TVMC_ERR_INVALID, "null table");
+    cudaStream_t st = as_stream(stream);
+    const bool dev = flags & TVMC_TRACE_DEVICE, rm = flags & TVMC_TRACE_ROW_MAJOR,
+               discard = flags & TVMC_DISCARD_LDE;
+    tvmc_commitment* c = new tvmc_commitment();
+    CK(cudaGetDevice(&c->device));
+    c->stream = st;
+    c->n = c->L = num_rows;
+    c->width = width;
+    c->pooled = true;
+    auto bail = [&](int code) {
+        tvmc_commitment_free(c);
+        return code;
+    };
+    const size_t NW = num_rows * width;
+    if (cudaMallocAsync((void**)&c->d_nodes, 2 * num_rows * 40, st) != cudaSuccess ||
+        cudaMemsetAsync(c->d_nodes, 0, 40, st) != cudaSuccess) {
+        cudaGetLastError();
+        return bail(fail(TVMC_ERR_NOMEM, "cannot allocate the tree of %zu leaves", num_rows));
+    }
+    // rows to hash, column-major: the caller's device table itself when it can be
+    // used as is and is not kept, else a copy the handle owns
+    const uint64_t* src = table;
+    if (width && !(dev && !rm && discard)) {
+        uint64_t* up = nullptr;
+        cudaError_t e = cudaMallocAsync((void**)&c->d_lde, NW * 8, st);
+        if (e == cudaSuccess && !dev && rm) {
+            e = cudaMallocAsync((void**)&up, NW * 8, st);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(up, table, NW * 8, cudaMemcpyHostToDevice, st);
+            if (e == cudaSuccess) e = launch_transpose(up, width, c->d_lde, num_rows, num_rows, width, st);
+        } else if (e == cudaSuccess && rm) {
+            e = launch_transpose(table, width, c->d_lde, num_rows, num_rows, width, st);
+        } else if (e == cudaSuccess) {
+            e = cudaMemcpyAsync(c->d_lde, table, NW * 8, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st);
+        }
+        if (up) cudaFreeAsync(up, st);
+        if (e != cudaSuccess) return bail(cuda_fail(e, "row upload"));
+        src = c->d_lde;
+    }
+    cudaError_t e = launch_hash_rows(src, 1, num_rows, num_rows, (uint32_t)width, nullptr, c->d_nodes, LAYOUT_HEAP, st);
+    if (e != cudaSuccess) return bail(cuda_fail(e, "hash/merkle"));
+    if (discard && c->d_lde) {
+        cudaFreeAsync(c->d_lde, st);
+        c->d_lde = nullptr;
+    }
+    return finish_commitment(c, flags, out);
+}
+
+int tvmc_commit_digests(const uint64_t* leaves, size_t num_leaves, uint32_t flags, void* stream,
+                        tvmc_commitment** out) {
+    if (!out) return fail(TVMC_ERR_INVALID, "null output handle");
+    *out = nullptr;
+    if (flags & ~(TVMC_TRACE_DEVICE | TVMC_LEAVES_XFE | TVMC_SYNC))
+        return fail(TVMC_ERR_INVALID, "unknown flag bits 0x%x", flags);
+    if (!is_pow2(num_leaves))
+        return fail(TVMC_ERR_INVALID, "Number of leaves must be a power of 2 (got %zu)", num_leaves);
+    if (!leaves) return fail(TVMC_ERR_INVALID, "null leaves");
+    cudaStream_t st = as_stream(stream);
+    const int words = (flags & TVMC_LEAVES_XFE) ? 3 : 5;
+    tvmc_commitment* c = new tvmc_commitment();
+    CK(cudaGetDevice(&c->device));
+    c->stream = st;
+    c->n = c->L = num_leaves;
+    c->width = 0;
+    c->pooled = true;
+    auto bail = [&](int code) {
+        tvmc_commitment_free(c);
+        return code;
+    };
+    if (cudaMallocAsync((void**)&c->d_nodes, 2 * num_leaves * 40, st) != cudaSuccess ||
+        cudaMemsetAsync(c->d_nodes, 0, 40, st) != cudaSuccess) {
+        cudaGetLastError();
+        return bail(fail(TVMC_ERR_NOMEM, "cannot allocate the tree of %zu leaves", num_leaves));
+    }
+    const uint64_t* src = leaves;
+    uint64_t* up = nullptr;
+    cudaError_t e = cudaSuccess;
+    if (!(flags & TVMC_TRACE_DEVICE)) {
+        e = cudaMallocAsync((void**)&up, num_leaves * words * 8, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(up, leaves, num_leaves * words * 8, cudaMemcpyHostToDevice, st);
+        src = up;
+    }
+    if (e == cudaSuccess) e = launch_merkle_tree(src, c->d_nodes, num_leaves, LAYOUT_HEAP, st, words);
+    if (up) cudaFreeAsync(up, st);
+    if (e != cudaSuccess) return bail(cuda_fail(e, "merkle"));
+    return finish_commitment(c, flags, out);
+}
+
 int tvmc_commitment_sync(tvmc_commitment* c) {
     if (!c) return fail(TVMC_ERR_INVALID, "null handle");
     CK(cudaEventSynchronize(c->done));

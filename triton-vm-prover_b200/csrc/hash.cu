@@ -190,13 +190,16 @@ __global__ void __launch_bounds__(HASH_THREADS) k_merkle_level(uint64_t* __restr
     store_digest(tree + 5 * node_slot(par, n, layout), h);
 }
 
+// Leaf i = the in_words words at leaves[in_words*i], zero-padded to a digest:
+// in_words = 5 copies digests, 3 turns an XFieldElement into the digest
+// (c0, c1, c2, 0, 0), as the reference's FRI trees do (src/fri/fri.cpp:25-43).
 __global__ void k_copy_leaves(const uint64_t* __restrict__ leaves, uint64_t* __restrict__ tree, uint64_t n,
-                              int layout) {
+                              int layout, int in_words) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     uint64_t* dst = tree + 5 * node_slot(n + i, n, layout);
 #pragma unroll
-    for (int k = 0; k < 5; k++) dst[k] = gl_canon(leaves[5 * i + k]);
+    for (int k = 0; k < 5; k++) dst[k] = k < in_words ? gl_canon(leaves[(uint64_t)in_words * i + k]) : 0;
 }
 
 __global__ void __launch_bounds__(128) k_hash_pairs(const uint64_t* __restrict__ left,
@@ -366,9 +369,9 @@ cudaError_t launch_hash_rows(const uint64_t* table, uint64_t rstride, uint64_t c
 }
 
 cudaError_t launch_merkle_tree(const uint64_t* leaves, uint64_t* tree, uint64_t n, int layout,
-                               cudaStream_t st) {
+                               cudaStream_t st, int leaf_words) {
     count_launch();
-    k_copy_leaves<<<grid_for(n, 256), 256, 0, st>>>(leaves, tree, n, layout);
+    k_copy_leaves<<<grid_for(n, 256), 256, 0, st>>>(leaves, tree, n, layout, leaf_words);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     return launch_merkle_from_leaves(tree, n, layout, st);

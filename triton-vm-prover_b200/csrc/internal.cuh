@@ -45,9 +45,10 @@ cudaError_t launch_hash_rows(const uint64_t* table, uint64_t rstride, uint64_t c
                              cudaStream_t st);
 // Complete a tree whose leaf level (n leaves) is already stored in `tree`.
 cudaError_t launch_merkle_from_leaves(uint64_t* tree, uint64_t n, int layout, cudaStream_t st);
-// Copy n leaf digests into the tree's leaf slots and complete the tree.
+// Copy n leaf digests into the tree's leaf slots and complete the tree.  With
+// leaf_words = 3 the leaves are XFieldElements, each padded to (c0, c1, c2, 0, 0).
 cudaError_t launch_merkle_tree(const uint64_t* leaves, uint64_t* tree, uint64_t n, int layout,
-                               cudaStream_t st);
+                               cudaStream_t st, int leaf_words = 5);
 // Frugal streaming: absorb ncols LDE columns (stride L) into per-row capacity
 // state cap[6][L]; `last` pads, finishes the digests as leaves of the heap tree
 // (2L digests) and builds the whole tree.

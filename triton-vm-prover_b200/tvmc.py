@@ -27,6 +27,7 @@ SYNC = 0x8
 PROFILE = 0x10
 FRUGAL = 0x20
 RAND_TRUNCATE = 0x40
+LEAVES_XFE = 0x80
 
 _u64p = ctypes.POINTER(ctypes.c_uint64)
 _szp = ctypes.POINTER(ctypes.c_size_t)
@@ -97,6 +98,8 @@ SIGNATURES = {
                                    ctypes.POINTER(_vp)]),
     "tvmc_commit_randomized": (ctypes.c_int, [_vp, _sz, _sz, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64,
                                               _vp, _sz, ctypes.c_uint32, _vp, ctypes.POINTER(_vp)]),
+    "tvmc_commit_rows": (ctypes.c_int, [_vp, _sz, _sz, ctypes.c_uint32, _vp, ctypes.POINTER(_vp)]),
+    "tvmc_commit_digests": (ctypes.c_int, [_vp, _sz, ctypes.c_uint32, _vp, ctypes.POINTER(_vp)]),
     "tvmc_commitment_root": (ctypes.c_int, [_vp, _u64p]),
     "tvmc_commitment_sync": (ctypes.c_int, [_vp]),
     "tvmc_commitment_shape": (ctypes.c_int, [_vp, _szp, _szp]),
@@ -407,6 +410,45 @@ class Commitment:
         self.width = width
         self.trace_len = trace_len
         self.lde_len = trace_len * expansion
+
+    @classmethod
+    def _wrap(cls, h, width, rows, keep=None):
+        obj = cls.__new__(cls)
+        obj.h, obj.width, obj.trace_len, obj.lde_len, obj._keep = h, width, rows, rows, keep
+        return obj
+
+    @classmethod
+    def from_rows(cls, table, row_major: bool = False, width: int | None = None, rows: int | None = None,
+                  device_ptr: bool = False, discard: bool = False, stream=None, sync: bool = False):
+        """tvmc_commit_rows: leaves = Tip5 hash of each row of an already evaluated
+        table (numpy (width, rows), or (rows, width) with row_major), no LDE."""
+        flags = (TRACE_ROW_MAJOR if row_major else 0) | (DISCARD_LDE if discard else 0) | (SYNC if sync else 0)
+        if device_ptr:
+            flags |= TRACE_DEVICE
+            ptr, keep = int(table), None
+        else:
+            t = _u64(table)
+            rows, width = t.shape if row_major else t.shape[::-1]
+            ptr, keep = (t.ctypes.data if t.size else None), t
+        h = _vp()
+        _check(lib().tvmc_commit_rows(ptr, rows, width, flags, _stream(stream), ctypes.byref(h)))
+        return cls._wrap(h, width, rows, keep)
+
+    @classmethod
+    def from_digests(cls, leaves, xfe: bool = False, count: int | None = None, device_ptr: bool = False,
+                     stream=None, sync: bool = False):
+        """tvmc_commit_digests: a tree over (n, 5) leaf digests, or with xfe=True over an
+        (n, 3) XFieldElement codeword (leaf = (c0, c1, c2, 0, 0))."""
+        flags = (LEAVES_XFE if xfe else 0) | (SYNC if sync else 0)
+        if device_ptr:
+            flags |= TRACE_DEVICE
+            ptr, keep = int(leaves), None
+        else:
+            lv = _u64(leaves).reshape(-1, 3 if xfe else 5)
+            count, ptr, keep = lv.shape[0], lv.ctypes.data, lv
+        h = _vp()
+        _check(lib().tvmc_commit_digests(ptr, count, flags, _stream(stream), ctypes.byref(h)))
+        return cls._wrap(h, 0, count, keep)
 
     def _h(self):
         if self.h is None:
