@@ -260,6 +260,16 @@ int tvmc_commit_rows(const uint64_t* table, size_t num_rows, size_t width, uint3
  * 715-730).  Host leaves, or device leaves with TVMC_TRACE_DEVICE; TVMC_SYNC. */
 int tvmc_commit_digests(const uint64_t* leaves, size_t num_leaves, uint32_t flags, void* stream,
                         tvmc_commitment** out);
+/* Fiat-Shamir absorb into a device sponge state (16 words; start from zeros):
+ * d_data[0..len) followed by 1 and zeros up to a multiple of 10, each 10-word
+ * chunk overwriting the rate, then one Tip5 permutation per chunk -- the
+ * reference's fs_absorb_device_gpu (src/gpu/kernels/fiat_shamir_kernel.cu:174-191)
+ * and ProofStream's pad-and-absorb, as one launch. */
+int tvmc_sponge_absorb_gpu(uint64_t* d_state, const uint64_t* d_data, size_t len, void* stream);
+/* Absorbs the commitment's root, encoded as the proof item MerkleRoot
+ * (discriminant 0, then the 5 root words), into d_state on `stream`, ordered
+ * after the commitment: the root never visits the host (src/gpu/gpu_stark.cu:2577-2585). */
+int tvmc_commitment_absorb_root(tvmc_commitment* c, uint64_t* d_state, void* stream);
 /* Wait for the commitment and copy its root (5 words) to host memory. */
 int tvmc_commitment_root(tvmc_commitment* c, uint64_t* root);
 int tvmc_commitment_sync(tvmc_commitment* c);

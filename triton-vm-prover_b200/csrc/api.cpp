@@ -1319,6 +1319,29 @@ int tvmc_commit_digests(const uint64_t* leaves, size_t num_leaves, uint32_t flag
     return finish_commitment(c, flags, out);
 }
 
+int tvmc_sponge_absorb_gpu(uint64_t* d_state, const uint64_t* d_data, size_t len, void* stream) {
+    if (!d_state || (len && !d_data)) return fail(TVMC_ERR_INVALID, "null argument");
+    CK(launch_sponge_absorb(d_state, d_data, len, 0, 0, as_stream(stream)));
+    return TVMC_OK;
+}
+
+int tvmc_commitment_absorb_root(tvmc_commitment* c, uint64_t* d_state, void* stream) {
+    if (!c || !d_state) return fail(TVMC_ERR_INVALID, "null argument");
+    cudaStream_t st = as_stream(stream);
+    CK(cudaStreamWaitEvent(st, c->done, 0));
+    // the proof item MerkleRoot: discriminant 0, then the root (heap node 1)
+    CK(launch_sponge_absorb(d_state, c->d_nodes + 5, 5, 1, 0, st));
+    if (st != c->stream) {  // a later free of the tree (on the commitment's stream) waits for this read
+        cudaEvent_t ev;
+        CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        cudaError_t e = cudaEventRecord(ev, st);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream, ev, 0);
+        cudaEventDestroy(ev);
+        CK(e);
+    }
+    return TVMC_OK;
+}
+
 int tvmc_commitment_sync(tvmc_commitment* c) {
     if (!c) return fail(TVMC_ERR_INVALID, "null handle");
     CK(cudaEventSynchronize(c->done));

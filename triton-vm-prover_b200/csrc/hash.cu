@@ -283,6 +283,36 @@ __global__ void __launch_bounds__(128) k_root_from_paths(const uint64_t* __restr
     for (int j = 0; j < 5; j++) roots[5 * q + j] = cur[j];
 }
 
+// Fiat-Shamir absorb into one device sponge state: the elements (an optional
+// leading word `lead`, then data[0..len)), then 1, then zeros to a multiple of
+// 10; each 10-word chunk overwrites the rate and is followed by a permutation.
+// One thread runs the chunks in order; the block only fills the S-box table.
+__global__ void __launch_bounds__(32) k_sponge_absorb(uint64_t* __restrict__ state, const uint64_t* __restrict__ data,
+                                                      uint64_t len, int has_lead, uint64_t lead) {
+    __shared__ uint32_t sbox[T5_SBOX_WORDS];
+    t5_sbox_init(sbox);
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    uint64_t s[T5_STATE];
+#pragma unroll
+    for (int i = 0; i < T5_STATE; i++) s[i] = state[i];
+    const uint64_t total = len + (has_lead ? 1 : 0);
+    const uint64_t padded = (total + T5_RATE) / T5_RATE * T5_RATE;  // room for the 1
+    for (uint64_t c0 = 0; c0 < padded; c0 += T5_RATE) {
+#pragma unroll
+        for (int i = 0; i < T5_RATE; i++) {
+            const uint64_t j = c0 + i;
+            uint64_t v = 0;
+            if (j < total) v = has_lead ? (j == 0 ? lead : data[j - 1]) : data[j];
+            else if (j == total) v = 1;
+            s[i] = gl_canon(v);
+        }
+        t5_permutation(s, sbox);
+    }
+#pragma unroll
+    for (int i = 0; i < T5_STATE; i++) state[i] = gl_canon(s[i]);
+}
+
 __global__ void k_gather_auth(const uint64_t* __restrict__ tree, uint64_t n, int layout, int height,
                               const uint64_t* __restrict__ idx, uint64_t count, uint64_t* __restrict__ out) {
     uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -404,6 +434,13 @@ cudaError_t launch_root_from_paths(const uint64_t* idx, const uint64_t* leaves, 
     if (count == 0) return cudaSuccess;
     count_launch();
     k_root_from_paths<<<grid_for(count, 128), 128, 0, st>>>(idx, leaves, paths, count, len, roots);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sponge_absorb(uint64_t* state, const uint64_t* data, uint64_t len, int has_lead, uint64_t lead,
+                                 cudaStream_t st) {
+    count_launch();
+    k_sponge_absorb<<<1, 32, 0, st>>>(state, data, len, has_lead, lead);
     return cudaGetLastError();
 }
 

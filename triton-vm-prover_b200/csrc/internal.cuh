@@ -57,6 +57,9 @@ cudaError_t launch_absorb_stripe(const uint64_t* stripe, uint64_t L, uint32_t nc
 cudaError_t launch_hash_pairs(const uint64_t* left, const uint64_t* right, uint64_t* out, uint64_t count,
                               cudaStream_t st);
 cudaError_t launch_tip5_permutations(uint64_t* states, uint64_t count, cudaStream_t st);
+// Fiat-Shamir absorb of [lead (if has_lead)] ++ data[0..len) into the 16-word sponge state.
+cudaError_t launch_sponge_absorb(uint64_t* state, const uint64_t* data, uint64_t len, int has_lead, uint64_t lead,
+                                 cudaStream_t st);
 // Tip5 rounds [r0, r0 + nr) of each state; trace (optional) gets the state after each round.
 cudaError_t launch_tip5_rounds(uint64_t* states, uint64_t count, int r0, int nr, uint64_t* trace, cudaStream_t st);
 // roots[q] = root implied by leaf digest leaves[q] at index idx[q] and its path of len siblings.

@@ -100,6 +100,8 @@ SIGNATURES = {
                                               _vp, _sz, ctypes.c_uint32, _vp, ctypes.POINTER(_vp)]),
     "tvmc_commit_rows": (ctypes.c_int, [_vp, _sz, _sz, ctypes.c_uint32, _vp, ctypes.POINTER(_vp)]),
     "tvmc_commit_digests": (ctypes.c_int, [_vp, _sz, ctypes.c_uint32, _vp, ctypes.POINTER(_vp)]),
+    "tvmc_sponge_absorb_gpu": (ctypes.c_int, [_vp, _vp, _sz, _vp]),
+    "tvmc_commitment_absorb_root": (ctypes.c_int, [_vp, _vp, _vp]),
     "tvmc_commitment_root": (ctypes.c_int, [_vp, _u64p]),
     "tvmc_commitment_sync": (ctypes.c_int, [_vp]),
     "tvmc_commitment_shape": (ctypes.c_int, [_vp, _szp, _szp]),
@@ -337,6 +339,10 @@ def lde_randomized_gpu(d_trace: int, cols: int, n: int, d_rnd: int, R: int, d_ou
                                          RAND_TRUNCATE if truncate else 0, _stream(stream)))
 
 
+def sponge_absorb_gpu(d_state: int, d_data: int, length: int, stream=None) -> None:
+    _check(lib().tvmc_sponge_absorb_gpu(d_state, d_data or None, length, _stream(stream)))
+
+
 def hash_rows_gpu(d_table: int, rows: int, cols: int, d_digests: int, stream=None) -> None:
     _check(lib().tvmc_hash_bfield_rows_gpu(d_table, rows, cols, d_digests, _stream(stream)))
 
@@ -454,6 +460,10 @@ class Commitment:
         if self.h is None:
             raise ValueError("commitment already freed")
         return self.h
+
+    def absorb_root(self, d_state: int, stream=None) -> None:
+        """Absorb the root (as proof item MerkleRoot) into a device sponge state."""
+        _check(lib().tvmc_commitment_absorb_root(self._h(), d_state, _stream(stream)))
 
     def sync(self) -> None:
         _check(lib().tvmc_commitment_sync(self._h()))
