@@ -82,37 +82,96 @@ __device__ __forceinline__ uint64_t t5_pow7(uint64_t x) {
     return gl_mul(x3, x4);
 }
 
-// Exact 32-bit <-> double conversions through the 2^52 exponent window.
-__device__ __forceinline__ double t5_u32_to_d(uint32_t v) {
-    return __hiloint2double(0x43300000, (int)v) - 4503599627370496.0;
-}
-__device__ __forceinline__ uint64_t t5_d_to_u52(double d) {
-    return (uint64_t)__double_as_longlong(d + 4503599627370496.0) & 0xFFFFFFFFFFFFFull;
+// Circulant MDS: out[r] = sum_c M[(r - c) mod 16] * s[c] (mod p), i.e. the
+// cyclic convolution m(x) s(x) mod x^16 - 1.  Each word is split into 32-bit
+// halves and each half is convolved exactly on the FP64 pipe, through the
+// factorisation x^16 - 1 = (x^4 - 1)(x^4 + 1)(x^8 + 1): the half is reduced
+// modulo each factor (additions), multiplied there by the matching reduction of
+// m (a cyclic 4-point, a negacyclic 4-point and a negacyclic 8-point product:
+// 96 DFMAs instead of the 256 of the direct product), and recombined by the
+// inverse of the same butterflies.  The halves enter centred (v - 2^31), so
+// every intermediate is an integer of magnitude at most 524757 * 2^33 < 2^53
+// (524757 = sum of the column, an upper bound on the l1 norm of every reduced
+// column), hence exact; the last FMA scales by 1/4 and adds back
+// 2^52 + 2^31 * 524757, leaving y + 2^52 with y < 2^52 the exact half-product.
+// The halves are then recombined as lo + hi*2^32 with one 128-bit reduction per
+// word.  Moving this work off the integer pipes leaves them to the S-box.
+__host__ __device__ __forceinline__ void t5_mds_half(double x[T5_STATE]) {
+    const double M[T5_STATE] = {TVMC_T5_MDS_FIRST_COLUMN};
+    double msum = 0.0;
+#pragma unroll
+    for (int k = 0; k < T5_STATE; k++) msum += M[k];
+    const double bias = 4503599627370496.0 + 2147483648.0 * msum;  // 2^52 + 2^31 * sum(M)
+    // reductions of the half modulo x^8 - 1 (a), x^8 + 1 (d), x^4 - 1 (e), x^4 + 1 (f)
+    double a[8], d[8], e[4], f[4];
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        a[j] = x[j] + x[j + 8];
+        d[j] = x[j] - x[j + 8];
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        e[j] = a[j] + a[j + 4];
+        f[j] = a[j] - a[j + 4];
+    }
+    // the same reductions of m: cyclic-4 c4, negacyclic-4 n4, negacyclic-8 n8
+    double P[4], Q[4], V[8];
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        double p = 0.0, q = 0.0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int i = (r - k) & 3;
+            const double c4 = M[i] + M[i + 4] + M[i + 8] + M[i + 12];
+            const double n4 = (M[i] + M[i + 8]) - (M[i + 4] + M[i + 12]);
+            p = fma(c4, e[k], p);
+            q = fma(k > r ? -n4 : n4, f[k], q);
+        }
+        P[r] = p;
+        Q[r] = q;
+    }
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+        double v = 0.0;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const int i = (r - k) & 7;
+            const double n8 = M[i] - M[i + 8];
+            v = fma(k > r ? -n8 : n8, d[k], v);
+        }
+        V[r] = v;
+    }
+    // inverse butterflies: 2u_r = P + Q, 2u_{r+4} = P - Q (u = result mod x^8 - 1),
+    // 4y_r = 2u_r + 2V_r, 4y_{r+8} = 2u_r - 2V_r
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        const double s = P[r] + Q[r], t = P[r] - Q[r];
+        x[r] = fma(fma(V[r], 2.0, s), 0.25, bias);
+        x[r + 8] = fma(fma(V[r], -2.0, s), 0.25, bias);
+        x[r + 4] = fma(fma(V[r + 4], 2.0, t), 0.25, bias);
+        x[r + 12] = fma(fma(V[r + 4], -2.0, t), 0.25, bias);
+    }
 }
 
-// Circulant MDS: out[r] = sum_c M[(r - c) mod 16] * s[c] (mod p).
-// Each word is split into 32-bit halves; the two 16x16 circulant products run
-// as DFMAs on the FP64 pipe, exact because every partial sum is an integer
-// below 524757 * 2^32 < 2^52 (524757 = sum of the column).  The halves are then
-// recombined as lo + hi*2^32 with one 128-bit reduction per word.  Moving this
-// work off the integer pipes leaves them to the S-box arithmetic.
+// A 32-bit half, centred: v - 2^31 exactly (the bits 0x43300000:v are 2^52 + v).
+constexpr double T5_HALF_BIAS = 4503599627370496.0 + 2147483648.0;  // 2^52 + 2^31
+__device__ __forceinline__ double t5_half_centred(uint32_t v) {
+    return __hiloint2double(0x43300000, (int)v) - T5_HALF_BIAS;
+}
+
 __device__ __forceinline__ void t5_mds(uint64_t s[T5_STATE]) {
-    const double M[T5_STATE] = {TVMC_T5_MDS_FIRST_COLUMN};
     double dl[T5_STATE], dh[T5_STATE];
 #pragma unroll
     for (int c = 0; c < T5_STATE; c++) {
-        dl[c] = t5_u32_to_d((uint32_t)s[c]);
-        dh[c] = t5_u32_to_d((uint32_t)(s[c] >> 32));
+        dl[c] = t5_half_centred((uint32_t)s[c]);
+        dh[c] = t5_half_centred((uint32_t)(s[c] >> 32));
     }
+    t5_mds_half(dl);
+    t5_mds_half(dh);
 #pragma unroll
     for (int r = 0; r < T5_STATE; r++) {
-        double al = 0.0, ah = 0.0;
-#pragma unroll
-        for (int c = 0; c < T5_STATE; c++) {
-            al = fma(M[(r - c) & 15], dl[c], al);
-            ah = fma(M[(r - c) & 15], dh[c], ah);
-        }
-        const uint64_t lo = t5_d_to_u52(al), hi = t5_d_to_u52(ah);
+        const uint64_t lo = (uint64_t)__double_as_longlong(dl[r]) & 0xFFFFFFFFFFFFFull;
+        const uint64_t hi = (uint64_t)__double_as_longlong(dh[r]) & 0xFFFFFFFFFFFFFull;
         // lo + hi*2^32 as a 128-bit number (sh:sl) with sh < 2^21
         const uint64_t sl = lo + (hi << 32);
         const uint64_t sh = (hi >> 32) + (uint64_t)(sl < lo);
