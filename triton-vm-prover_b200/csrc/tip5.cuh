@@ -13,7 +13,9 @@
 //     owning its own bank, so the 8 lookups per word never conflict;
 //   * the MDS runs exactly on the FP64 pipe (t5_mds), in parallel with the
 //     integer S-box work on the ALU/FMA pipes;
-//   * x^7 is a rolled loop over three groups of four words.
+//   * x^7 is a rolled loop over three groups of four words, its products
+//     reduced on the ALU (gl_mul_alu): the 32-bit multiply-adds of the
+//     products alone keep the multiply-add pipe the busiest one.
 #pragma once
 #include <cstdint>
 #include "field.cuh"
@@ -76,10 +78,10 @@ __device__ __forceinline__ uint64_t t5_split_lookup(uint64_t x, const uint32_t* 
 }
 
 __device__ __forceinline__ uint64_t t5_pow7(uint64_t x) {
-    uint64_t x2 = gl_sqr(x);
-    uint64_t x3 = gl_mul(x, x2);
-    uint64_t x4 = gl_sqr(x2);
-    return gl_mul(x3, x4);
+    uint64_t x2 = gl_mul_alu(x, x);
+    uint64_t x3 = gl_mul_alu(x, x2);
+    uint64_t x4 = gl_mul_alu(x2, x2);
+    return gl_mul_alu(x3, x4);
 }
 
 // Circulant MDS: out[r] = sum_c M[(r - c) mod 16] * s[c] (mod p), i.e. the
