@@ -57,6 +57,28 @@ __device__ __forceinline__ void gl_mul128(uint64_t a, uint64_t b, uint32_t& r0, 
         : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
 }
 
+// a^2 as four 32-bit limbs with three partial products: the cross term a0*a1
+// is formed once and doubled on the ALU (into 65 bits), which saves one 32-bit
+// multiply and one high multiply against gl_mul128(a, a).
+__device__ __forceinline__ void gl_sqr128(uint64_t a, uint32_t& r0, uint32_t& r1, uint32_t& r2, uint32_t& r3) {
+    const uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32);
+    asm("{\n\t"
+        ".reg .u32 t1, m0, m1, d2;\n\t"
+        "mul.lo.u32 %0, %4, %4;\n\t"
+        "mul.hi.u32 t1, %4, %4;\n\t"
+        "mul.lo.u32 m0, %4, %5;\n\t"
+        "mul.hi.u32 m1, %4, %5;\n\t"
+        "add.cc.u32 m0, m0, m0;\n\t"
+        "addc.cc.u32 m1, m1, m1;\n\t"
+        "addc.u32 d2, 0, 0;\n\t"
+        "add.cc.u32 %1, t1, m0;\n\t"
+        "madc.lo.cc.u32 %2, %5, %5, m1;\n\t"
+        "madc.hi.u32 %3, %5, %5, d2;\n\t"
+        "}"
+        : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+        : "r"(a0), "r"(a1));
+}
+
 // (r3:r2:r1:r0) -> (r1:r0) + r2*(2^32-1) - r3 (mod p) as a 64-bit
 // representative (2^64 = 2^32 - 1 and 2^96 = -1 mod p).  The first sum is two
 // multiply-adds (on the FMA pipe) with carry c in {0, 1}; subtracting r3 leaves
@@ -121,6 +143,13 @@ __device__ __forceinline__ uint64_t gl_mul(uint64_t a, uint64_t b) {
 __device__ __forceinline__ uint64_t gl_mul_c(uint64_t a, uint64_t b) { return gl_canon(gl_mul(a, b)); }
 
 __device__ __forceinline__ uint64_t gl_sqr(uint64_t a) { return gl_mul(a, a); }
+
+// a^2 through gl_sqr128, reduced on the ALU; partial result.
+__device__ __forceinline__ uint64_t gl_sqr_alu(uint64_t a) {
+    uint32_t r0, r1, r2, r3;
+    gl_sqr128(a, r0, r1, r2, r3);
+    return gl_reduce_limbs_alu(r0, r1, r2, r3);
+}
 
 // a * b with the reduction on the ALU (gl_reduce_limbs_alu); partial result.
 __device__ __forceinline__ uint64_t gl_mul_alu(uint64_t a, uint64_t b) {

@@ -78,9 +78,9 @@ __device__ __forceinline__ uint64_t t5_split_lookup(uint64_t x, const uint32_t* 
 }
 
 __device__ __forceinline__ uint64_t t5_pow7(uint64_t x) {
-    uint64_t x2 = gl_mul_alu(x, x);
+    uint64_t x2 = gl_sqr_alu(x);
     uint64_t x3 = gl_mul_alu(x, x2);
-    uint64_t x4 = gl_mul_alu(x2, x2);
+    uint64_t x4 = gl_sqr_alu(x2);
     return gl_mul_alu(x3, x4);
 }
 
