@@ -216,6 +216,77 @@ __device__ __forceinline__ uint64_t gl_sub_c(uint64_t a, uint64_t b) {
     return ((uint64_t)r1 << 32) | r0;
 }
 
+// ---- multiplication by powers of two -------------------------------------
+// 2 has order 192 mod p (2^96 = -1), so every root of unity of order <= 64 is
+// +-2^s with s < 96: a shift and a short reduction instead of a multiply.  The
+// shift amounts below must be constants after inlining and unrolling (the
+// branches on them then fold away).
+
+// x * 2^s for 0 < s <= 32 and any 64-bit x: lo + hi*(2^32 - 1) with hi < 2^32
+// (carry c in {0, 1}, folded as c*(2^32 - 1) without a second carry); partial.
+__device__ __forceinline__ uint64_t gl_shl_le32(uint64_t x, int s) {
+    const uint32_t x0 = (uint32_t)x, x1 = (uint32_t)(x >> 32);
+    const uint32_t lo0 = s == 32 ? 0u : x0 << s;
+    const uint32_t lo1 = s == 32 ? x0 : __funnelshift_l(x0, x1, s);
+    const uint32_t hi = s == 32 ? x1 : x1 >> (32 - s);
+    uint32_t r0, r1;
+    asm("{\n\t"
+        ".reg .u32 c;\n\t"
+        "mad.lo.cc.u32 %0, %4, 0xFFFFFFFF, %2;\n\t"
+        "madc.hi.cc.u32 %1, %4, 0xFFFFFFFF, %3;\n\t"
+        "addc.u32 c, 0, 0;\n\t"
+        "neg.s32 c, c;\n\t"
+        "add.cc.u32 %0, %0, c;\n\t"
+        "addc.u32 %1, %1, 0;\n\t"
+        "}"
+        : "=r"(r0), "=r"(r1)
+        : "r"(lo0), "r"(lo1), "r"(hi));
+    return ((uint64_t)r1 << 32) | r0;
+}
+
+// x * 2^s for 32 < s < 64: the 128-bit shift reduced by gl_reduce_limbs; partial.
+__device__ __forceinline__ uint64_t gl_shl_gt32(uint64_t x, int s) {
+    const uint32_t x0 = (uint32_t)x, x1 = (uint32_t)(x >> 32);
+    return gl_reduce_limbs(0u, x0 << (s - 32), __funnelshift_r(x0, x1, 64 - s), x1 >> (64 - s));
+}
+
+// x * 2^-k for 0 < k <= 32 and canonical x, canonical: with x = q*2^k + r,
+// x * 2^-k = q + r*2^(32-k) * 2^-32 and 2^-32 = 1 - 2^32 (mod p), so the
+// result is u - t*2^32 with t = r*2^(32-k) < 2^32 and u = q + t < 2^63 + 2^32;
+// a borrow adds p back (subtracts 2^32 - 1 modulo 2^64) and cannot recur.
+__device__ __forceinline__ uint64_t gl_shr_c(uint64_t x, int k) {
+    const uint32_t x0 = (uint32_t)x, x1 = (uint32_t)(x >> 32);
+    const uint32_t q0 = k == 32 ? x1 : __funnelshift_r(x0, x1, k);
+    const uint32_t q1 = k == 32 ? 0u : x1 >> k;
+    const uint32_t t = k == 32 ? x0 : x0 << (32 - k);
+    uint32_t r0, r1;
+    asm("{\n\t"
+        ".reg .u32 u0, u1, m;\n\t"
+        "add.cc.u32 u0, %2, %4;\n\t"
+        "addc.u32 u1, %3, 0;\n\t"
+        "sub.cc.u32 %1, u1, %4;\n\t"
+        "subc.u32 m, 0, 0;\n\t"
+        "sub.cc.u32 %0, u0, m;\n\t"
+        "subc.u32 %1, %1, 0;\n\t"
+        "}"
+        : "=r"(r0), "=r"(r1)
+        : "r"(q0), "r"(q1), "r"(t));
+    return ((uint64_t)r1 << 32) | r0;
+}
+
+// (a - c) * 2^e for canonical a, c and 0 <= e < 192; canonical.  A negative
+// factor (2^e = -2^(e-96), and 2^s = -2^-(96-s)) swaps the subtraction.
+__device__ __forceinline__ uint64_t gl_sub_mul_pow2_c(uint64_t a, uint64_t c, int e) {
+    bool neg = e >= 96;
+    const int s = neg ? e - 96 : e;
+    if (s >= 64) neg = !neg;
+    const uint64_t d = neg ? gl_sub_c(c, a) : gl_sub_c(a, c);
+    if (s == 0) return d;
+    if (s <= 32) return gl_canon(gl_shl_le32(d, s));
+    if (s < 64) return gl_canon(gl_shl_gt32(d, s));
+    return gl_shr_c(d, 96 - s);
+}
+
 __device__ __forceinline__ uint64_t gl_pow(uint64_t b, uint64_t e) {
     uint64_t r = 1;
     while (e) {

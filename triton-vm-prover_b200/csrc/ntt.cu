@@ -65,9 +65,18 @@ __device__ __forceinline__ constexpr int brevc(int k) {
     return r;
 }
 
+// The forward 32-point root w_32 = 7^((p-1)/32) is 2^78 (mod p); every root of
+// order 2^m <= 32 is its power 2^(78 * 2^(5-m) mod 192).
+constexpr int GL_W32_LOG2 = 78;
+
 // Radix-2 DIF network on R = 2^B registers; X[k] ends in v[brev(k)].
 // tw[e] = w^e for the 2^LS-point root w, so w_{2h}^j = tw[j * 2^LS / 2h].
-template <int LS, int B>
+// With P2 the network is the forward one (w = the forward root) and its
+// twiddles w_{2h}^j, roots of order <= 32, are applied as powers of two
+// (gl_sub_mul_pow2_c) without reading tw.  An inverse transform runs through
+// the same network on index-negated input: DFT_{w^-1}(x)[k] = DFT_w(x')[k]
+// with x'[i] = x[-i mod n].
+template <int LS, int B, bool P2 = false>
 __device__ __forceinline__ void reg_dft(uint64_t (&v)[1 << B], const uint64_t* tw) {
 #pragma unroll
     for (int st = 0; st < B; st++) {
@@ -79,8 +88,12 @@ __device__ __forceinline__ void reg_dft(uint64_t (&v)[1 << B], const uint64_t* t
             for (int j = 0; j < h; j++) {
                 const uint64_t a = v[blk + j], c = v[blk + j + h];
                 v[blk + j] = gl_add_c(a, c);
-                const uint64_t d = gl_sub_c(a, c);
-                v[blk + j + h] = j == 0 ? d : gl_mul_c(d, tw[j << (LS - B + st)]);
+                if constexpr (P2) {
+                    v[blk + j + h] = gl_sub_mul_pow2_c(a, c, (GL_W32_LOG2 * j * (16 / h)) % 192);
+                } else {
+                    const uint64_t d = gl_sub_c(a, c);
+                    v[blk + j + h] = j == 0 ? d : gl_mul_c(d, tw[j << (LS - B + st)]);
+                }
             }
         }
     }
@@ -94,8 +107,9 @@ __device__ __forceinline__ void reg_dft(uint64_t (&v)[1 << B], const uint64_t* t
 // after a __syncthreads().  s is a shared buffer of spad_words(2^LS, lT) words
 // for the transposes between rounds and tw holds w^e, e < 2^LS.  Callers must
 // __syncthreads() before reusing s or before reading, in another thread,
-// anything a store wrote to shared memory.
-template <int LS, bool TO_SMEM = false, class LoadF, class StoreF>
+// anything a store wrote to shared memory.  P2: forward root, register rounds
+// with power-of-two twiddles (reg_dft).
+template <int LS, bool TO_SMEM = false, bool P2 = false, class LoadF, class StoreF>
 __device__ __forceinline__ void sub_dft(uint64_t* s, int lT, const uint64_t* tw, LoadF&& load, StoreF&& store) {
     using PL = Plan<LS>;
     const int T = 1 << lT;
@@ -105,7 +119,7 @@ __device__ __forceinline__ void sub_dft(uint64_t* s, int lT, const uint64_t* tw,
             uint64_t v[R];
 #pragma unroll
             for (int j = 0; j < R; j++) v[j] = load(j, t);
-            reg_dft<LS, LS>(v, tw);
+            reg_dft<LS, LS, P2>(v, tw);
 #pragma unroll
             for (int k = 0; k < R; k++) {
                 if constexpr (TO_SMEM) s[spos(k, lT) + t] = v[brevc<LS>(k)];
@@ -120,7 +134,7 @@ __device__ __forceinline__ void sub_dft(uint64_t* s, int lT, const uint64_t* tw,
             uint64_t v[R2];
 #pragma unroll
             for (int j = 0; j < R2; j++) v[j] = load(d1 + (j << b1), t);
-            reg_dft<LS, b2>(v, tw);
+            reg_dft<LS, b2, P2>(v, tw);
 #pragma unroll
             for (int k2 = 0; k2 < R2; k2++) {
                 uint64_t x = v[brevc<b2>(k2)];
@@ -135,7 +149,7 @@ __device__ __forceinline__ void sub_dft(uint64_t* s, int lT, const uint64_t* tw,
             uint64_t v[R1];
 #pragma unroll
             for (int d1 = 0; d1 < R1; d1++) v[d1] = s[spos(d1 + (k2 << b1), lT) + t];
-            reg_dft<LS, b1>(v, tw);
+            reg_dft<LS, b1, P2>(v, tw);
 #pragma unroll
             for (int k1 = 0; k1 < R1; k1++) {
                 if constexpr (TO_SMEM) s[spos(k1 + (k2 << b1), lT) + t] = v[brevc<b1>(k1)];
@@ -151,7 +165,7 @@ __device__ __forceinline__ void sub_dft(uint64_t* s, int lT, const uint64_t* tw,
             uint64_t v[R3];
 #pragma unroll
             for (int j = 0; j < R3; j++) v[j] = load(lo + (j << (b1 + b2)), t);
-            reg_dft<LS, b3>(v, tw);
+            reg_dft<LS, b3, P2>(v, tw);
 #pragma unroll
             for (int k3 = 0; k3 < R3; k3++) {
                 uint64_t x = v[brevc<b3>(k3)];
@@ -169,7 +183,7 @@ __device__ __forceinline__ void sub_dft(uint64_t* s, int lT, const uint64_t* tw,
             uint64_t v[R2];
 #pragma unroll
             for (int j = 0; j < R2; j++) v[j] = s[spos(base + (j << b1), lT) + t];
-            reg_dft<LS, b2>(v, tw);
+            reg_dft<LS, b2, P2>(v, tw);
 #pragma unroll
             for (int k2 = 0; k2 < R2; k2++) {
                 uint64_t x = v[brevc<b2>(k2)];
@@ -186,7 +200,7 @@ __device__ __forceinline__ void sub_dft(uint64_t* s, int lT, const uint64_t* tw,
             uint64_t v[R1];
 #pragma unroll
             for (int d1 = 0; d1 < R1; d1++) v[d1] = s[spos(d1 + (rest << b1), lT) + t];
-            reg_dft<LS, b1>(v, tw);
+            reg_dft<LS, b1, P2>(v, tw);
 #pragma unroll
             for (int k1 = 0; k1 < R1; k1++) {
                 if constexpr (TO_SMEM) s[spos(k1 + (rest << b1), lT) + t] = v[brevc<b1>(k1)];
@@ -327,25 +341,28 @@ __global__ void __launch_bounds__(NTT_THREADS) k_lde_small(const uint64_t* trace
     }
 }
 
-// K1: inverse pass A over the trace: Y[i1 + n1*k2] = w^-(i1*k2) DFT^-1_n2(...)[k2].
+// K1: inverse pass A over the trace: Y[i1 + n1*k2] = w^-(i1*k2) DFT^-1_n2(...)[k2],
+// the inverse DFT taken as the forward one of the index-negated column (reg_dft).
 // At 2^10-point passes the unbounded allocation takes 136 registers (one
 // 256-thread CTA per SM); capping it at two CTAs per SM is 4% faster on the
 // 2^20-row LDE.  The other kernels keep their unbounded allocations, which
 // measured faster than capped ones.
 template <int L2>
 __global__ void __launch_bounds__(NTT_THREADS, L2 == 10 ? 2 : 1) k_lde_inv_a(const uint64_t* trace, uint64_t tld, uint64_t* Y,
-                                                           uint64_t yld, int l1, int lT, const uint64_t* tw12_i,
+                                                           uint64_t yld, int l1, int lT, const uint64_t* tw12_f,
                                                            const uint64_t* wlo, const uint64_t* whi) {
     extern __shared__ uint64_t sm[];
     uint64_t* tw = sm;
     uint64_t* s = sm + (1 << L2);
-    load_tw<L2>(tw, tw12_i);
+    load_tw<L2>(tw, tw12_f);
     __syncthreads();
     const uint32_t i10 = blockIdx.x << lT;
     const uint64_t* src = trace + (uint64_t)blockIdx.y * tld + i10;
     uint64_t* dst = Y + (uint64_t)blockIdx.y * yld + i10;
-    sub_dft<L2, true>(
-        s, lT, tw, [&](int k, int t) { return gl_canon(src[t + ((uint64_t)k << l1)]); }, [](int, int, uint64_t) {});
+    constexpr int n2m = (1 << L2) - 1;
+    sub_dft<L2, true, true>(
+        s, lT, tw, [&](int k, int t) { return gl_canon(src[t + ((uint64_t)(-k & n2m) << l1)]); },
+        [](int, int, uint64_t) {});
     __syncthreads();
     const int T = 1 << lT;
     for (int idx = threadIdx.x; idx < (T << L2); idx += blockDim.x) {
@@ -372,14 +389,13 @@ __global__ void __launch_bounds__(NTT_THREADS) k_lde_mid(const uint64_t* Y, uint
     uint64_t* twf = twi + n1;
     uint64_t* cf = twf + n1;                 // coefficients, natural k1 order
     uint64_t* s = cf + spad_words(n1, lT);   // transposes
-    load_tw<L1>(twi, tw12_i);
-    load_tw<L1>(twf, tw12_f);
+    load_tw<L1>(twf, tw12_f);  // the inverse also runs on the forward root (slot twi unused)
     __syncthreads();
     const uint64_t col = blockIdx.y;
     const uint32_t k20 = blockIdx.x << lT;
     const uint64_t* src = Y + col * yld + ((uint64_t)k20 << L1);
-    sub_dft<L1>(
-        s, lT, twi, [&](int k, int t) { return src[((uint64_t)t << L1) + k]; },
+    sub_dft<L1, false, true>(  // inverse: forward DFT of the index-negated row
+        s, lT, twf, [&](int k, int t) { return src[((uint64_t)t << L1) + (-k & (n1 - 1))]; },
         [&](int k, int t, uint64_t v) { cf[spos(k, lT) + t] = v; });
     __syncthreads();
     const uint64_t N = 1ull << (L1 + l2);
@@ -387,7 +403,7 @@ __global__ void __launch_bounds__(NTT_THREADS) k_lde_mid(const uint64_t* Y, uint
         const uint64_t* lo = sc_lo + 4096 * c;
         const uint64_t* hi = sc_hi + hi_len * c;
         uint64_t* dst = Z + (col * E + c) * N + k20;
-        sub_dft<L1, true>(
+        sub_dft<L1, true, true>(
             s, lT, twf,
             [&](int k, int t) {
                 uint64_t x = cf[spos(k, lT) + t];
@@ -430,8 +446,7 @@ __global__ void __launch_bounds__(128) k_lde_mid_reg(const uint64_t* Y, uint64_t
     uint64_t* twi = sm;
     uint64_t* twf = twi + n1;
     uint64_t* s = twf + n1;
-    load_tw<L1>(twi, tw12_i);
-    load_tw<L1>(twf, tw12_f);
+    load_tw<L1>(twf, tw12_f);  // the inverse also runs on the forward root (slot twi unused)
     __syncthreads();
     const int E = 1 << le;
     const uint64_t col = blockIdx.y;
@@ -442,12 +457,12 @@ __global__ void __launch_bounds__(128) k_lde_mid_reg(const uint64_t* Y, uint64_t
         const int t = id & (T - 1), d1 = id >> lT;
         uint64_t v[R2];
 #pragma unroll
-        for (int j = 0; j < R2; j++) v[j] = src[((uint64_t)t << L1) + d1 + (j << b1)];
-        reg_dft<L1, b2>(v, twi);
+        for (int j = 0; j < R2; j++) v[j] = src[((uint64_t)t << L1) + (-(d1 + (j << b1)) & (n1 - 1))];
+        reg_dft<L1, b2, true>(v, twf);  // inverse as the forward DFT of the index-negated row
 #pragma unroll
         for (int k2 = 0; k2 < R2; k2++) {
             uint64_t x = v[brevc<b2>(k2)];
-            if (k2) x = gl_mul_c(x, twi[d1 * k2]);
+            if (k2) x = gl_mul_c(x, twf[d1 * k2]);
             s[spos(d1 + (k2 << b1), lT) + t] = x;
         }
     }
@@ -459,7 +474,7 @@ __global__ void __launch_bounds__(128) k_lde_mid_reg(const uint64_t* Y, uint64_t
         uint64_t v[R1];
 #pragma unroll
         for (int d1 = 0; d1 < R1; d1++) v[d1] = s[spos(d1 + (kk << b1), lT) + t];
-        reg_dft<L1, b1>(v, twi);
+        reg_dft<L1, b1, true>(v, twf);
 #pragma unroll
         for (int k1 = 0; k1 < R1; k1++) cf[k1] = v[brevc<b1>(k1)];
     }
@@ -481,7 +496,7 @@ __global__ void __launch_bounds__(128) k_lde_mid_reg(const uint64_t* Y, uint64_t
                 }
                 v[k1] = gl_mul_c(x, tw2(lo, hi, i));
             }
-            reg_dft<L1, b1>(v, twf);
+            reg_dft<L1, b1, true>(v, twf);
 #pragma unroll
             for (int q = 0; q < R1; q++) {
                 uint64_t x = v[brevc<b1>(q)];
@@ -496,7 +511,7 @@ __global__ void __launch_bounds__(128) k_lde_mid_reg(const uint64_t* Y, uint64_t
             uint64_t w[R2];
 #pragma unroll
             for (int i1 = 0; i1 < R2; i1++) w[i1] = s[spos(i1 + (q2 << b2), lT) + tt];
-            reg_dft<L1, b2>(w, twf);
+            reg_dft<L1, b2, true>(w, twf);
 #pragma unroll
             for (int q1 = 0; q1 < R2; q1++) s[spos(q1 + (q2 << b2), lT) + tt] = w[brevc<b2>(q1)];
         }
@@ -530,8 +545,7 @@ __global__ void __launch_bounds__(128, MINB) k_lde_mid_sym(const uint64_t* Y, ui
     uint64_t* twi = sm;
     uint64_t* twf = twi + n1;
     uint64_t* s = twf + n1;
-    load_tw<L1>(twi, tw12_i);
-    load_tw<L1>(twf, tw12_f);
+    load_tw<L1>(twf, tw12_f);  // the inverse also runs on the forward root (slot twi unused)
     __syncthreads();
     const int E = 1 << le;
     const uint64_t col = blockIdx.y;
@@ -542,16 +556,16 @@ __global__ void __launch_bounds__(128, MINB) k_lde_mid_sym(const uint64_t* Y, ui
     uint64_t cf[R];  // coefficients c[R*k1 + ln] of row k20 + t
 #pragma unroll 1
     for (int pass = 0; pass <= E; pass++) {  // 0: inverse; c + 1: forward, coset c
-        const uint64_t* tw = pass ? twf : twi;
+        const uint64_t* tw = twf;  // the inverse runs forward on the index-negated row
         const uint64_t* lo = sc_lo + 4096 * (pass ? pass - 1 : 0);
         const uint64_t* hi = sc_hi + hi_len * (pass ? pass - 1 : 0);
 #pragma unroll 1
         for (int half = 0; half < 2; half++) {
             uint64_t v[R];
             if (half == 0) {
-                if (pass == 0) {  // inverse round 1: elements ln + R*j of row t
+                if (pass == 0) {  // inverse round 1: elements -(ln + R*j) of row t
 #pragma unroll
-                    for (int j = 0; j < R; j++) v[j] = src[((uint64_t)t << L1) + ln + (j << B)];
+                    for (int j = 0; j < R; j++) v[j] = src[((uint64_t)t << L1) + (-(ln + (j << B)) & (n1 - 1))];
                 } else {  // forward round 1: c[ln + R*k1] * N^-1 s_c^i
 #pragma unroll
                     for (int k1 = 0; k1 < R; k1++) {
@@ -568,7 +582,7 @@ __global__ void __launch_bounds__(128, MINB) k_lde_mid_sym(const uint64_t* Y, ui
 #pragma unroll
                 for (int x = 0; x < R; x++) v[x] = s[spos(x + (ln << B), lT) + t];
             }
-            reg_dft<L1, B>(v, tw);
+            reg_dft<L1, B, true>(v, tw);
             if (half == 0) {  // twiddle w^(ln*k), slot ln + R*k
 #pragma unroll
                 for (int k = 0; k < R; k++) {
@@ -615,7 +629,7 @@ __global__ void __launch_bounds__(NTT_THREADS) k_lde_fwd_b(const uint64_t* Z, ui
     const uint64_t N = 1ull << (l1 + L2);
     const uint64_t* src = Z + col * E * N + ((uint64_t)q20 << L2);
     uint64_t* dst = out + col * old + (uint64_t)q20 * E;
-    sub_dft<L2>(
+    sub_dft<L2, false, true>(
         s, lS, tw,
         [&](int k, int u) {
             const int c = u & (E - 1), t = u >> le;
@@ -813,7 +827,7 @@ cudaError_t launch_lde(const LdePlan& pl, const uint64_t* trace, uint64_t tld, u
             if (e2 != cudaSuccess) return e2;
             count_launch();
             k_lde_inv_a<L2><<<dim3((1u << l1) >> lT1, nc), NTT_THREADS, smem1, st>>>(
-                trace + c0 * tld, tld, Y, N, l1, lT1, pl.tw12_i, pl.wn_i_lo, pl.wn_i_hi);
+                trace + c0 * tld, tld, Y, N, l1, lT1, pl.tw12_f, pl.wn_i_lo, pl.wn_i_hi);
             return cudaGetLastError();
         });
         if (e != cudaSuccess) return e;
