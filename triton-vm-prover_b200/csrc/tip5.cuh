@@ -13,9 +13,11 @@
 //     owning its own bank, so the 8 lookups per word never conflict;
 //   * the MDS runs exactly on the FP64 pipe (t5_mds), in parallel with the
 //     integer S-box work on the ALU/FMA pipes;
-//   * x^7 is a rolled loop over three groups of four words, its products
-//     reduced on the ALU (gl_mul_alu): the 32-bit multiply-adds of the
-//     products alone keep the multiply-add pipe the busiest one.
+//   * x^7 is a rolled loop over three groups of four words; three of its four
+//     products are reduced on the ALU (gl_sqr_alu, gl_mul_alu) and the squares
+//     take three partial products, which balances the ALU and multiply-add
+//     pipes (the 32-bit multiply-adds of the products alone would keep the
+//     multiply-add pipe the busier one).
 #pragma once
 #include <cstdint>
 #include "field.cuh"
@@ -81,7 +83,7 @@ __device__ __forceinline__ uint64_t t5_pow7(uint64_t x) {
     uint64_t x2 = gl_sqr_alu(x);
     uint64_t x3 = gl_mul_alu(x, x2);
     uint64_t x4 = gl_sqr_alu(x2);
-    return gl_mul_alu(x3, x4);
+    return gl_mul(x3, x4);  // reduced on the multiply-add pipe: the two pipes balance
 }
 
 // Circulant MDS: out[r] = sum_c M[(r - c) mod 16] * s[c] (mod p), i.e. the
