@@ -69,15 +69,13 @@ __device__ __forceinline__ constexpr int brevc(int k) {
 // order 2^m <= 32 is its power 2^(78 * 2^(5-m) mod 192).
 constexpr int GL_W32_LOG2 = 78;
 
-// Radix-2 DIF network on R = 2^B registers; X[k] ends in v[brev(k)].
-// tw[e] = w^e for the 2^LS-point root w, so w_{2h}^j = tw[j * 2^LS / 2h].
-// With P2 the network is the forward one (w = the forward root) and its
-// twiddles w_{2h}^j, roots of order <= 32, are applied as powers of two
-// (gl_sub_mul_pow2_c) without reading tw.  An inverse transform runs through
-// the same network on index-negated input: DFT_{w^-1}(x)[k] = DFT_w(x')[k]
-// with x'[i] = x[-i mod n].
-template <int LS, int B, bool P2 = false>
-__device__ __forceinline__ void reg_dft(uint64_t (&v)[1 << B], const uint64_t* tw) {
+// Radix-2 DIF network on R = 2^B registers (forward root); X[k] ends in
+// v[brev(k)].  Its twiddles w_{2h}^j are roots of order <= 32, applied as
+// powers of two (gl_sub_mul_pow2_c): no table, no general multiply.  Every
+// inverse transform here runs through the same forward networks on
+// index-negated input: DFT_{w^-1}(x)[k] = DFT_w(x')[k] with x'[i] = x[-i mod n].
+template <int B>
+__device__ __forceinline__ void reg_dft(uint64_t (&v)[1 << B]) {
 #pragma unroll
     for (int st = 0; st < B; st++) {
         constexpr int R = 1 << B;
@@ -88,12 +86,7 @@ __device__ __forceinline__ void reg_dft(uint64_t (&v)[1 << B], const uint64_t* t
             for (int j = 0; j < h; j++) {
                 const uint64_t a = v[blk + j], c = v[blk + j + h];
                 v[blk + j] = gl_add_c(a, c);
-                if constexpr (P2) {
-                    v[blk + j + h] = gl_sub_mul_pow2_c(a, c, (GL_W32_LOG2 * j * (16 / h)) % 192);
-                } else {
-                    const uint64_t d = gl_sub_c(a, c);
-                    v[blk + j + h] = j == 0 ? d : gl_mul_c(d, tw[j << (LS - B + st)]);
-                }
+                v[blk + j + h] = gl_sub_mul_pow2_c(a, c, (GL_W32_LOG2 * j * (16 / h)) % 192);
             }
         }
     }
@@ -107,9 +100,10 @@ __device__ __forceinline__ void reg_dft(uint64_t (&v)[1 << B], const uint64_t* t
 // after a __syncthreads().  s is a shared buffer of spad_words(2^LS, lT) words
 // for the transposes between rounds and tw holds w^e, e < 2^LS.  Callers must
 // __syncthreads() before reusing s or before reading, in another thread,
-// anything a store wrote to shared memory.  P2: forward root, register rounds
-// with power-of-two twiddles (reg_dft).
-template <int LS, bool TO_SMEM = false, bool P2 = false, class LoadF, class StoreF>
+// anything a store wrote to shared memory.  The transform is the forward one
+// (tw holds powers of the forward root; callers negate input indices for an
+// inverse).
+template <int LS, bool TO_SMEM = false, class LoadF, class StoreF>
 __device__ __forceinline__ void sub_dft(uint64_t* s, int lT, const uint64_t* tw, LoadF&& load, StoreF&& store) {
     using PL = Plan<LS>;
     const int T = 1 << lT;
@@ -119,7 +113,7 @@ __device__ __forceinline__ void sub_dft(uint64_t* s, int lT, const uint64_t* tw,
             uint64_t v[R];
 #pragma unroll
             for (int j = 0; j < R; j++) v[j] = load(j, t);
-            reg_dft<LS, LS, P2>(v, tw);
+            reg_dft<LS>(v);
 #pragma unroll
             for (int k = 0; k < R; k++) {
                 if constexpr (TO_SMEM) s[spos(k, lT) + t] = v[brevc<LS>(k)];
@@ -134,7 +128,7 @@ __device__ __forceinline__ void sub_dft(uint64_t* s, int lT, const uint64_t* tw,
             uint64_t v[R2];
 #pragma unroll
             for (int j = 0; j < R2; j++) v[j] = load(d1 + (j << b1), t);
-            reg_dft<LS, b2, P2>(v, tw);
+            reg_dft<b2>(v);
 #pragma unroll
             for (int k2 = 0; k2 < R2; k2++) {
                 uint64_t x = v[brevc<b2>(k2)];
@@ -149,7 +143,7 @@ __device__ __forceinline__ void sub_dft(uint64_t* s, int lT, const uint64_t* tw,
             uint64_t v[R1];
 #pragma unroll
             for (int d1 = 0; d1 < R1; d1++) v[d1] = s[spos(d1 + (k2 << b1), lT) + t];
-            reg_dft<LS, b1, P2>(v, tw);
+            reg_dft<b1>(v);
 #pragma unroll
             for (int k1 = 0; k1 < R1; k1++) {
                 if constexpr (TO_SMEM) s[spos(k1 + (k2 << b1), lT) + t] = v[brevc<b1>(k1)];
@@ -165,7 +159,7 @@ __device__ __forceinline__ void sub_dft(uint64_t* s, int lT, const uint64_t* tw,
             uint64_t v[R3];
 #pragma unroll
             for (int j = 0; j < R3; j++) v[j] = load(lo + (j << (b1 + b2)), t);
-            reg_dft<LS, b3, P2>(v, tw);
+            reg_dft<b3>(v);
 #pragma unroll
             for (int k3 = 0; k3 < R3; k3++) {
                 uint64_t x = v[brevc<b3>(k3)];
@@ -183,7 +177,7 @@ __device__ __forceinline__ void sub_dft(uint64_t* s, int lT, const uint64_t* tw,
             uint64_t v[R2];
 #pragma unroll
             for (int j = 0; j < R2; j++) v[j] = s[spos(base + (j << b1), lT) + t];
-            reg_dft<LS, b2, P2>(v, tw);
+            reg_dft<b2>(v);
 #pragma unroll
             for (int k2 = 0; k2 < R2; k2++) {
                 uint64_t x = v[brevc<b2>(k2)];
@@ -200,7 +194,7 @@ __device__ __forceinline__ void sub_dft(uint64_t* s, int lT, const uint64_t* tw,
             uint64_t v[R1];
 #pragma unroll
             for (int d1 = 0; d1 < R1; d1++) v[d1] = s[spos(d1 + (rest << b1), lT) + t];
-            reg_dft<LS, b1, P2>(v, tw);
+            reg_dft<b1>(v);
 #pragma unroll
             for (int k1 = 0; k1 < R1; k1++) {
                 if constexpr (TO_SMEM) s[spos(k1 + (rest << b1), lT) + t] = v[brevc<b1>(k1)];
@@ -239,8 +233,10 @@ __device__ __forceinline__ void load_tw(uint64_t* tw, const uint64_t* __restrict
 
 // ---------------------------------------------------------------- plain NTT
 
-// Whole columns per CTA: T = 2^lT columns, size 2^LS <= 2^11, in place.
-template <int LS>
+// Whole columns per CTA: T = 2^lT columns, size 2^LS <= 2^11, in place.  All
+// transforms run on the forward root (tw12 = w_4096 powers); INV negates the
+// input index, which turns the forward DFT into the inverse one (reg_dft).
+template <int LS, bool INV>
 __global__ void __launch_bounds__(NTT_THREADS) k_ntt_small(uint64_t* data, uint64_t ld, uint64_t cols, int lT,
                                                            const uint64_t* tw12, uint64_t scale) {
     extern __shared__ uint64_t sm[];
@@ -249,16 +245,18 @@ __global__ void __launch_bounds__(NTT_THREADS) k_ntt_small(uint64_t* data, uint6
     load_tw<LS>(tw, tw12);
     __syncthreads();
     const uint64_t c0 = (uint64_t)blockIdx.x << lT;
+    constexpr int nm = (1 << LS) - 1;
     sub_dft<LS>(
         s, lT, tw,
-        [&](int k, int t) { return c0 + t < cols ? gl_canon(data[(c0 + t) * ld + k]) : 0ull; },
+        [&](int k, int t) { return c0 + t < cols ? gl_canon(data[(c0 + t) * ld + (INV ? -k & nm : k)]) : 0ull; },
         [&](int k, int t, uint64_t v) {
             if (c0 + t < cols) data[(c0 + t) * ld + k] = gl_mul_c(v, scale);
         });
 }
 
 // Pass A: out[i1 + n1*k2] = w^(i1*k2) * DFT_n2(in[i1 + n1*i2])[k2]; in may equal out.
-template <int L2>
+// tw12 is the forward table; INV: inverse sub-DFT (negated input index).
+template <int L2, bool INV>
 __global__ void __launch_bounds__(NTT_THREADS) k_pass_a(const uint64_t* in, uint64_t ild, uint64_t* out,
                                                         uint64_t old, int l1, int lT, const uint64_t* tw12,
                                                         const uint64_t* wlo, const uint64_t* whi) {
@@ -270,8 +268,10 @@ __global__ void __launch_bounds__(NTT_THREADS) k_pass_a(const uint64_t* in, uint
     const uint32_t i10 = blockIdx.x << lT;
     const uint64_t* src = in + (uint64_t)blockIdx.y * ild + i10;
     uint64_t* dst = out + (uint64_t)blockIdx.y * old + i10;
+    constexpr int n2m = (1 << L2) - 1;
     sub_dft<L2, true>(
-        s, lT, tw, [&](int k, int t) { return gl_canon(src[t + ((uint64_t)k << l1)]); }, [](int, int, uint64_t) {});
+        s, lT, tw, [&](int k, int t) { return gl_canon(src[t + ((uint64_t)(INV ? -k & n2m : k) << l1)]); },
+        [](int, int, uint64_t) {});
     __syncthreads();
     const int T = 1 << lT;
     for (int idx = threadIdx.x; idx < (T << L2); idx += blockDim.x) {
@@ -282,7 +282,8 @@ __global__ void __launch_bounds__(NTT_THREADS) k_pass_a(const uint64_t* in, uint
 }
 
 // Pass B: out[n2*k1 + k2] = scale * DFT_n1(in[i1 + n1*k2])[k1]; in != out.
-template <int L1>
+// tw12 is the forward table; INV: inverse sub-DFT (negated input index).
+template <int L1, bool INV>
 __global__ void __launch_bounds__(NTT_THREADS) k_pass_b(const uint64_t* in, uint64_t ild, uint64_t* out,
                                                         uint64_t old, int l2, int lT, const uint64_t* tw12,
                                                         uint64_t scale) {
@@ -294,8 +295,9 @@ __global__ void __launch_bounds__(NTT_THREADS) k_pass_b(const uint64_t* in, uint
     const uint32_t k20 = blockIdx.x << lT;
     const uint64_t* src = in + (uint64_t)blockIdx.y * ild + ((uint64_t)k20 << L1);
     uint64_t* dst = out + (uint64_t)blockIdx.y * old + k20;
+    constexpr int n1m = (1 << L1) - 1;
     sub_dft<L1>(
-        s, lT, tw, [&](int k, int t) { return src[((uint64_t)t << L1) + k]; },
+        s, lT, tw, [&](int k, int t) { return src[((uint64_t)t << L1) + (INV ? -k & n1m : k)]; },
         [&](int k, int t, uint64_t v) { dst[((uint64_t)k << l2) + t] = gl_mul_c(v, scale); });
 }
 
@@ -311,17 +313,16 @@ __global__ void __launch_bounds__(NTT_THREADS) k_lde_small(const uint64_t* trace
     extern __shared__ uint64_t sm[];
     constexpr int n = 1 << LS;
     const int E = 1 << le;
-    uint64_t* twi = sm;
+    uint64_t* twi = sm;                    // (unused: the inverse runs on the forward root)
     uint64_t* twf = twi + n;
     uint64_t* cf = twf + n;                // coefficients (natural order)
     uint64_t* s = cf + spad_words(n, lT);  // transposes
-    load_tw<LS>(twi, tw12_i);
     load_tw<LS>(twf, tw12_f);
     __syncthreads();
     const uint64_t c0 = (uint64_t)blockIdx.x << lT;
-    sub_dft<LS>(
-        s, lT, twi,
-        [&](int k, int t) { return c0 + t < cols ? gl_canon(trace[(c0 + t) * tld + k]) : 0ull; },
+    sub_dft<LS>(  // inverse: forward DFT of the index-negated column
+        s, lT, twf,
+        [&](int k, int t) { return c0 + t < cols ? gl_canon(trace[(c0 + t) * tld + (-k & (n - 1))]) : 0ull; },
         [&](int k, int t, uint64_t v) { cf[spos(k, lT) + t] = v; });
     __syncthreads();
     for (int c = 0; c < E; c++) {
@@ -360,7 +361,7 @@ __global__ void __launch_bounds__(NTT_THREADS, L2 == 10 ? 2 : 1) k_lde_inv_a(con
     const uint64_t* src = trace + (uint64_t)blockIdx.y * tld + i10;
     uint64_t* dst = Y + (uint64_t)blockIdx.y * yld + i10;
     constexpr int n2m = (1 << L2) - 1;
-    sub_dft<L2, true, true>(
+    sub_dft<L2, true>(
         s, lT, tw, [&](int k, int t) { return gl_canon(src[t + ((uint64_t)(-k & n2m) << l1)]); },
         [](int, int, uint64_t) {});
     __syncthreads();
@@ -394,7 +395,7 @@ __global__ void __launch_bounds__(NTT_THREADS) k_lde_mid(const uint64_t* Y, uint
     const uint64_t col = blockIdx.y;
     const uint32_t k20 = blockIdx.x << lT;
     const uint64_t* src = Y + col * yld + ((uint64_t)k20 << L1);
-    sub_dft<L1, false, true>(  // inverse: forward DFT of the index-negated row
+    sub_dft<L1>(  // inverse: forward DFT of the index-negated row
         s, lT, twf, [&](int k, int t) { return src[((uint64_t)t << L1) + (-k & (n1 - 1))]; },
         [&](int k, int t, uint64_t v) { cf[spos(k, lT) + t] = v; });
     __syncthreads();
@@ -403,7 +404,7 @@ __global__ void __launch_bounds__(NTT_THREADS) k_lde_mid(const uint64_t* Y, uint
         const uint64_t* lo = sc_lo + 4096 * c;
         const uint64_t* hi = sc_hi + hi_len * c;
         uint64_t* dst = Z + (col * E + c) * N + k20;
-        sub_dft<L1, true, true>(
+        sub_dft<L1, true>(
             s, lT, twf,
             [&](int k, int t) {
                 uint64_t x = cf[spos(k, lT) + t];
@@ -458,7 +459,7 @@ __global__ void __launch_bounds__(128) k_lde_mid_reg(const uint64_t* Y, uint64_t
         uint64_t v[R2];
 #pragma unroll
         for (int j = 0; j < R2; j++) v[j] = src[((uint64_t)t << L1) + (-(d1 + (j << b1)) & (n1 - 1))];
-        reg_dft<L1, b2, true>(v, twf);  // inverse as the forward DFT of the index-negated row
+        reg_dft<b2>(v);  // inverse as the forward DFT of the index-negated row
 #pragma unroll
         for (int k2 = 0; k2 < R2; k2++) {
             uint64_t x = v[brevc<b2>(k2)];
@@ -474,7 +475,7 @@ __global__ void __launch_bounds__(128) k_lde_mid_reg(const uint64_t* Y, uint64_t
         uint64_t v[R1];
 #pragma unroll
         for (int d1 = 0; d1 < R1; d1++) v[d1] = s[spos(d1 + (kk << b1), lT) + t];
-        reg_dft<L1, b1, true>(v, twf);
+        reg_dft<b1>(v);
 #pragma unroll
         for (int k1 = 0; k1 < R1; k1++) cf[k1] = v[brevc<b1>(k1)];
     }
@@ -496,7 +497,7 @@ __global__ void __launch_bounds__(128) k_lde_mid_reg(const uint64_t* Y, uint64_t
                 }
                 v[k1] = gl_mul_c(x, tw2(lo, hi, i));
             }
-            reg_dft<L1, b1, true>(v, twf);
+            reg_dft<b1>(v);
 #pragma unroll
             for (int q = 0; q < R1; q++) {
                 uint64_t x = v[brevc<b1>(q)];
@@ -511,7 +512,7 @@ __global__ void __launch_bounds__(128) k_lde_mid_reg(const uint64_t* Y, uint64_t
             uint64_t w[R2];
 #pragma unroll
             for (int i1 = 0; i1 < R2; i1++) w[i1] = s[spos(i1 + (q2 << b2), lT) + tt];
-            reg_dft<L1, b2, true>(w, twf);
+            reg_dft<b2>(w);
 #pragma unroll
             for (int q1 = 0; q1 < R2; q1++) s[spos(q1 + (q2 << b2), lT) + tt] = w[brevc<b2>(q1)];
         }
@@ -582,7 +583,7 @@ __global__ void __launch_bounds__(128, MINB) k_lde_mid_sym(const uint64_t* Y, ui
 #pragma unroll
                 for (int x = 0; x < R; x++) v[x] = s[spos(x + (ln << B), lT) + t];
             }
-            reg_dft<L1, B, true>(v, tw);
+            reg_dft<B>(v);
             if (half == 0) {  // twiddle w^(ln*k), slot ln + R*k
 #pragma unroll
                 for (int k = 0; k < R; k++) {
@@ -629,7 +630,7 @@ __global__ void __launch_bounds__(NTT_THREADS) k_lde_fwd_b(const uint64_t* Z, ui
     const uint64_t N = 1ull << (l1 + L2);
     const uint64_t* src = Z + col * E * N + ((uint64_t)q20 << L2);
     uint64_t* dst = out + col * old + (uint64_t)q20 * E;
-    sub_dft<L2, false, true>(
+    sub_dft<L2>(
         s, lS, tw,
         [&](int k, int u) {
             const int c = u & (E - 1), t = u >> le;
@@ -733,7 +734,7 @@ size_t ntt_scratch_words(int logn, uint64_t cols) { return logn <= 11 ? 0 : (siz
 cudaError_t launch_ntt(const LdePlan& pl, int inverse, uint64_t* data, uint64_t ld, uint64_t cols,
                        uint64_t* scratch, cudaStream_t st) {
     const int l = pl.logn;
-    const uint64_t* tw12 = inverse ? pl.tw12_i : pl.tw12_f;
+    const uint64_t* tw12 = pl.tw12_f;  // the inverse negates the sub-DFT input indices instead
     const uint64_t scale = (inverse && l > 0) ? GL_P - ((GL_P - 1) >> l) : 1;  // n^-1 = p - (p-1)/n
     if (cols == 0 || l == 0) return cudaSuccess;  // size-1 transform is the identity
     if (l <= 11) {
@@ -741,11 +742,11 @@ cudaError_t launch_ntt(const LdePlan& pl, int inverse, uint64_t* data, uint64_t 
         const int T = 1 << lT;
         const size_t smem = words_bytes((1u << l) + spad_words(1 << l, lT));
         return dispatch_ls(l, [&]<int LS>() -> cudaError_t {
-            cudaError_t e = set_smem((const void*)k_ntt_small<LS>, smem);
+            auto kern = inverse ? k_ntt_small<LS, true> : k_ntt_small<LS, false>;
+            cudaError_t e = set_smem((const void*)kern, smem);
             if (e != cudaSuccess) return e;
             count_launch();
-            k_ntt_small<LS><<<(unsigned)((cols + T - 1) / T), NTT_THREADS, smem, st>>>(data, ld, cols, lT, tw12,
-                                                                                      scale);
+            kern<<<(unsigned)((cols + T - 1) / T), NTT_THREADS, smem, st>>>(data, ld, cols, lT, tw12, scale);
             return cudaGetLastError();
         });
     }
@@ -759,20 +760,22 @@ cudaError_t launch_ntt(const LdePlan& pl, int inverse, uint64_t* data, uint64_t 
     for (uint64_t c0 = 0; c0 < cols; c0 += 65535) {
         const unsigned nc = (unsigned)((cols - c0) < 65535 ? (cols - c0) : 65535);
         cudaError_t e = dispatch_ls(l2, [&]<int L2>() -> cudaError_t {
-            cudaError_t e2 = set_smem((const void*)k_pass_a<L2>, smem_a);
+            auto kern = inverse ? k_pass_a<L2, true> : k_pass_a<L2, false>;
+            cudaError_t e2 = set_smem((const void*)kern, smem_a);
             if (e2 != cudaSuccess) return e2;
             count_launch();
-            k_pass_a<L2><<<dim3((1u << l1) >> lTa, nc), NTT_THREADS, smem_a, st>>>(data + c0 * ld, ld, scratch, n,
-                                                                                  l1, lTa, tw12, wlo, whi);
+            kern<<<dim3((1u << l1) >> lTa, nc), NTT_THREADS, smem_a, st>>>(data + c0 * ld, ld, scratch, n, l1, lTa,
+                                                                          tw12, wlo, whi);
             return cudaGetLastError();
         });
         if (e != cudaSuccess) return e;
         e = dispatch_ls(l1, [&]<int L1>() -> cudaError_t {
-            cudaError_t e2 = set_smem((const void*)k_pass_b<L1>, smem_b);
+            auto kern = inverse ? k_pass_b<L1, true> : k_pass_b<L1, false>;
+            cudaError_t e2 = set_smem((const void*)kern, smem_b);
             if (e2 != cudaSuccess) return e2;
             count_launch();
-            k_pass_b<L1><<<dim3((1u << l2) >> lTb, nc), NTT_THREADS, smem_b, st>>>(scratch, n, data + c0 * ld, ld,
-                                                                                  l2, lTb, tw12, scale);
+            kern<<<dim3((1u << l2) >> lTb, nc), NTT_THREADS, smem_b, st>>>(scratch, n, data + c0 * ld, ld, l2, lTb,
+                                                                          tw12, scale);
             return cudaGetLastError();
         });
         if (e != cudaSuccess) return e;
