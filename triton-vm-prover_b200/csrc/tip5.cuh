@@ -62,21 +62,46 @@ __device__ __forceinline__ uint32_t t5_lookup32(uint32_t m, const uint32_t* lane
     return __byte_perm(lo, hi, 0x5410);
 }
 
-// split_and_lookup (src/hash/tip5.cpp:119-145) for any representative x.
+// split_and_lookup (src/hash/tip5.cpp:119-145) for any representative x; the
+// result is a representative in [1, p] (p for zero), which the MDS accepts.
+// Both Montgomery conversions are 32-bit carry chains:
+//   in:  x * 2^64 = x0*(2^32 - 1) - x1 (mod p) for x = x1*2^32 + x0: the
+//        difference (x0*2^32 - x0) - x1 is canonical, or wraps once and is
+//        corrected by adding p (subtracting 2^32 - 1 modulo 2^64);
+//   out: y * 2^-64 = p - b with b = a - (a >> 32) - [a < y] (mod 2^64) and
+//        a = y + (y << 32) (mod 2^64), the reduction of y by the Montgomery
+//        factor p^-1 = 2^32 + 1 (mod 2^64).
 __device__ __forceinline__ uint64_t t5_split_lookup(uint64_t x, const uint32_t* lane_tbl) {
-    // Montgomery form x * 2^64 mod p = x0*(2^32-1) - x1 (mod p), always canonical.
-    uint64_t x0 = x & GL_EPS, x1 = x >> 32;
-    uint64_t t = (x0 << 32) - x0;
-    uint64_t m = t - x1;
-    if (t < x1) m -= GL_EPS;
-    uint32_t lo = t5_lookup32((uint32_t)m, lane_tbl);
-    uint32_t hi = t5_lookup32((uint32_t)(m >> 32), lane_tbl);
-    uint64_t y = ((uint64_t)hi << 32) | lo;
-    // back from Montgomery form: y * 2^-64 mod p, canonical.
-    uint64_t sh = y << 32;
-    uint64_t a = y + sh;
-    uint64_t b = a - (a >> 32) - (uint64_t)(a < y);
-    return b ? GL_P - b : 0;
+    uint32_t m0, m1;
+    asm("{\n\t"
+        ".reg .u32 t0, t1, k;\n\t"
+        "sub.cc.u32 t0, 0, %2;\n\t"
+        "subc.u32 t1, %2, 0;\n\t"
+        "sub.cc.u32 %0, t0, %3;\n\t"
+        "subc.cc.u32 %1, t1, 0;\n\t"
+        "subc.u32 k, 0, 0;\n\t"
+        "sub.cc.u32 %0, %0, k;\n\t"
+        "subc.u32 %1, %1, 0;\n\t"
+        "}"
+        : "=r"(m0), "=r"(m1)
+        : "r"((uint32_t)x), "r"((uint32_t)(x >> 32)));
+    const uint32_t y0 = t5_lookup32(m0, lane_tbl);
+    const uint32_t y1 = t5_lookup32(m1, lane_tbl);
+    uint32_t r0, r1;
+    asm("{\n\t"
+        ".reg .u32 a1, c, b0, b1;\n\t"
+        "add.cc.u32 a1, %3, %2;\n\t"
+        "addc.u32 c, 0, 0;\n\t"
+        "sub.cc.u32 b0, %2, a1;\n\t"
+        "subc.u32 b1, a1, 0;\n\t"
+        "sub.cc.u32 b0, b0, c;\n\t"
+        "subc.u32 b1, b1, 0;\n\t"
+        "sub.cc.u32 %0, 1, b0;\n\t"
+        "subc.u32 %1, 0xFFFFFFFF, b1;\n\t"
+        "}"
+        : "=r"(r0), "=r"(r1)
+        : "r"(y0), "r"(y1));
+    return ((uint64_t)r1 << 32) | r0;
 }
 
 __device__ __forceinline__ uint64_t t5_pow7(uint64_t x) {
