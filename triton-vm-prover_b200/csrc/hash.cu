@@ -54,7 +54,7 @@ __global__ void __launch_bounds__(HASH_THREADS, HASH_CTAS_PER_SM) k_hash_rows(
     const uint64_t* __restrict__ tab, uint64_t rstride, uint64_t cstride, uint64_t rows, uint32_t width,
     uint64_t* __restrict__ digests, uint64_t* __restrict__ tree, int layout, int fuse) {
     __shared__ uint32_t sbox[T5_SBOX_WORDS];
-    __shared__ uint64_t sd[HASH_THREADS * 5];
+    extern __shared__ uint64_t sd[];  // 5 * blockDim words when fuse > 0 (fused tree levels), else none
     t5_sbox_init(sbox);
     __syncthreads();
     const uint32_t* lt = sbox + (threadIdx.x & 31);
@@ -112,7 +112,7 @@ __global__ void __launch_bounds__(HASH_THREADS, HASH_CTAS_PER_SM) k_absorb_strip
     const uint64_t* __restrict__ stripe, uint64_t L, uint32_t ncols, uint64_t* __restrict__ cap, int first,
     int last, uint64_t* __restrict__ tree, int fuse) {
     __shared__ uint32_t sbox[T5_SBOX_WORDS];
-    __shared__ uint64_t sd[HASH_THREADS * 5];
+    extern __shared__ uint64_t sd[];  // 5 * blockDim words when fuse > 0 (fused tree levels), else none
     t5_sbox_init(sbox);
     __syncthreads();
     const uint32_t* lt = sbox + (threadIdx.x & 31);
@@ -395,8 +395,8 @@ cudaError_t launch_hash_rows(const uint64_t* table, uint64_t rstride, uint64_t c
     unsigned threads = (unsigned)(rows < HASH_THREADS ? rows : HASH_THREADS);
     const int fuse = ilog2u(threads) < tuning_hash_fuse_levels() ? ilog2u(threads) : tuning_hash_fuse_levels();
     count_launch();
-    k_hash_rows<<<grid_for(rows, threads), threads, 0, st>>>(table, rstride, cstride, rows, width, nullptr, tree,
-                                                             layout, fuse);
+    k_hash_rows<<<grid_for(rows, threads), threads, fuse > 0 ? 40 * threads : 0, st>>>(
+        table, rstride, cstride, rows, width, nullptr, tree, layout, fuse);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     // the block subtrees are complete up to `fuse` levels; continue from there
@@ -480,7 +480,8 @@ cudaError_t launch_absorb_stripe(const uint64_t* stripe, uint64_t L, uint32_t nc
     const int lt = 63 - __builtin_clzll(threads);
     const int fuse = last ? (lt < tuning_hash_fuse_levels() ? lt : tuning_hash_fuse_levels()) : 0;
     count_launch();
-    k_absorb_stripe<<<(unsigned)(L / threads), threads, 0, st>>>(stripe, L, ncols, cap, first, last, tree, fuse);
+    k_absorb_stripe<<<(unsigned)(L / threads), threads, fuse > 0 ? 40 * threads : 0, st>>>(stripe, L, ncols, cap,
+                                                                                          first, last, tree, fuse);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess || !last) return e;
     return launch_tree_above(tree, L, L >> fuse, LAYOUT_HEAP, st);  // complete the tree above the block subtrees

@@ -9,8 +9,10 @@
 //
 // B200 layout choices (measured on sm_100a: 32-bit IMAD and DFMA are
 // half-rate, IMAD.HI quarter-rate, IMAD.WIDE takes two issue slots):
-//   * the byte table lives in shared memory as 64 words x 32 lanes, every lane
-//     owning its own bank, so the 8 lookups per word never conflict;
+//   * the byte table lives in shared memory as 256 words x 32 lanes, one
+//     entry per word and every lane owning its own bank, so the 8 lookups per
+//     word never conflict and the looked-up bytes are assembled by byte
+//     permutes with constant selectors;
 //   * the MDS runs exactly on the FP64 pipe (t5_mds), in parallel with the
 //     integer S-box work on the ALU/FMA pipes;
 //   * x^7 is a rolled loop over three groups of four words; three of its four
@@ -33,33 +35,28 @@ constexpr int T5_ROUNDS = 5;
 // in t5_mds below as FP64 literals.
 __device__ __constant__ uint64_t c_t5_rc[T5_ROUNDS * T5_STATE] = {TVMC_T5_ROUND_CONSTANTS};
 
-// Shared-memory S-box table: word w of lane l holds table bytes 4w..4w+3.
-constexpr int T5_SBOX_WORDS = 64 * 32;
+// Shared-memory S-box table (32 KB): word v*32 + l holds the table byte for
+// input byte v, in lane l's private column.
+constexpr int T5_SBOX_WORDS = 256 * 32;
 
 // Fill the lane-replicated byte table; call from all threads, then sync.
 __device__ __forceinline__ void t5_sbox_init(uint32_t* tbl) {
     for (int i = threadIdx.x; i < T5_SBOX_WORDS; i += blockDim.x) {
-        int w = i >> 5;
-        uint32_t v = 0;
-        for (int b = 0; b < 4; b++) {
-            int x = 4 * w + b + 1;
-            int c = (x * x % 257) * x % 257;
-            v |= (uint32_t)((c + 256) % 257) << (8 * b);
-        }
-        tbl[i] = v;
+        const int x = (i >> 5) + 1;
+        const int c = (x * x % 257) * x % 257;
+        tbl[i] = (uint32_t)((c + 256) % 257);
     }
 }
 
-// Byte-wise S-box of a 32-bit word through the lane's private table column.
+// Byte-wise S-box of a 32-bit word through the lane's private table column:
+// each lookup returns its byte in bits 0-7, so the assembly is three byte
+// permutes with constant selectors.
 __device__ __forceinline__ uint32_t t5_lookup32(uint32_t m, const uint32_t* lane_tbl) {
-    uint32_t w0 = lane_tbl[((m >> 2) & 63) << 5];
-    uint32_t w1 = lane_tbl[((m >> 10) & 63) << 5];
-    uint32_t w2 = lane_tbl[((m >> 18) & 63) << 5];
-    uint32_t w3 = lane_tbl[((m >> 26) & 63) << 5];
-    // byte k of the result = byte (m_k & 3) of w_k
-    uint32_t lo = __byte_perm(w0, w1, (m & 3) | (((m >> 8) & 3) + 4) << 4);
-    uint32_t hi = __byte_perm(w2, w3, ((m >> 16) & 3) | (((m >> 24) & 3) + 4) << 4);
-    return __byte_perm(lo, hi, 0x5410);
+    const uint32_t w0 = lane_tbl[(m & 255) << 5];
+    const uint32_t w1 = lane_tbl[((m >> 8) & 255) << 5];
+    const uint32_t w2 = lane_tbl[((m >> 16) & 255) << 5];
+    const uint32_t w3 = lane_tbl[(m >> 24) << 5];
+    return __byte_perm(__byte_perm(w0, w1, 0x0040), __byte_perm(w2, w3, 0x0040), 0x5410);
 }
 
 // split_and_lookup (src/hash/tip5.cpp:119-145) for any representative x; the
