@@ -31,9 +31,32 @@ constexpr int T5_STATE = 16;
 constexpr int T5_RATE = 10;
 constexpr int T5_ROUNDS = 5;
 
-// Round constants of Tip5 (tip5_params.h).  The MDS first column is inlined
-// in t5_mds below as FP64 literals.
-__device__ __constant__ uint64_t c_t5_rc[T5_ROUNDS * T5_STATE] = {TVMC_T5_ROUND_CONSTANTS};
+// The MDS first column is inlined in t5_mds_half as FP64 literals.  The round
+// constants (tip5_params.h) enter the MDS's last FMA (t5_mds): the biases
+// below carry each constant's 32-bit halves.
+constexpr double t5_mds_column_sum() {
+    const double m[T5_STATE] = {TVMC_T5_MDS_FIRST_COLUMN};
+    double acc = 0.0;
+    for (int k = 0; k < T5_STATE; k++) acc += m[k];
+    return acc;
+}
+// 2^52 + 2^31 * sum(M): the output bias of a centred half-product (t5_mds_half).
+constexpr double T5_MDS_BIAS = 4503599627370496.0 + 2147483648.0 * t5_mds_column_sum();
+
+struct T5RoundBias {
+    double lo[T5_ROUNDS * T5_STATE];  // T5_MDS_BIAS + (rc & (2^32 - 1))
+    double hi[T5_ROUNDS * T5_STATE];  // T5_MDS_BIAS + (rc >> 32)
+};
+constexpr T5RoundBias t5_round_bias() {
+    const uint64_t rc[T5_ROUNDS * T5_STATE] = {TVMC_T5_ROUND_CONSTANTS};
+    T5RoundBias b{};
+    for (int i = 0; i < T5_ROUNDS * T5_STATE; i++) {
+        b.lo[i] = T5_MDS_BIAS + (double)(uint32_t)rc[i];
+        b.hi[i] = T5_MDS_BIAS + (double)(uint32_t)(rc[i] >> 32);
+    }
+    return b;
+}
+__device__ __constant__ T5RoundBias c_t5_bias = t5_round_bias();
 
 // Shared-memory S-box table (32 KB): word v*32 + l holds the table byte for
 // input byte v, in lane l's private column.
@@ -118,16 +141,13 @@ __device__ __forceinline__ uint64_t t5_pow7(uint64_t x) {
 // inverse of the same butterflies.  The halves enter centred (v - 2^31), so
 // every intermediate is an integer of magnitude at most 524757 * 2^33 < 2^53
 // (524757 = sum of the column, an upper bound on the l1 norm of every reduced
-// column), hence exact; the last FMA scales by 1/4 and adds back
-// 2^52 + 2^31 * 524757, leaving y + 2^52 with y < 2^52 the exact half-product.
+// column), hence exact; the last FMA scales by 1/4 and adds bias[r] =
+// T5_MDS_BIAS + a[r] (2^52 + 2^31 * 524757 undoes the centring; a[r] < 2^32 is
+// the round constant's half), leaving y + a + 2^52 with y + a < 2^52 exact.
 // The halves are then recombined as lo + hi*2^32 with one 128-bit reduction per
 // word.  Moving this work off the integer pipes leaves them to the S-box.
-__host__ __device__ __forceinline__ void t5_mds_half(double x[T5_STATE]) {
+__host__ __device__ __forceinline__ void t5_mds_half(double x[T5_STATE], const double* bias) {
     const double M[T5_STATE] = {TVMC_T5_MDS_FIRST_COLUMN};
-    double msum = 0.0;
-#pragma unroll
-    for (int k = 0; k < T5_STATE; k++) msum += M[k];
-    const double bias = 4503599627370496.0 + 2147483648.0 * msum;  // 2^52 + 2^31 * sum(M)
     // reductions of the half modulo x^8 - 1 (a), x^8 + 1 (d), x^4 - 1 (e), x^4 + 1 (f)
     double a[8], d[8], e[4], f[4];
 #pragma unroll
@@ -172,10 +192,10 @@ __host__ __device__ __forceinline__ void t5_mds_half(double x[T5_STATE]) {
 #pragma unroll
     for (int r = 0; r < 4; r++) {
         const double s = P[r] + Q[r], t = P[r] - Q[r];
-        x[r] = fma(fma(V[r], 2.0, s), 0.25, bias);
-        x[r + 8] = fma(fma(V[r], -2.0, s), 0.25, bias);
-        x[r + 4] = fma(fma(V[r + 4], 2.0, t), 0.25, bias);
-        x[r + 12] = fma(fma(V[r + 4], -2.0, t), 0.25, bias);
+        x[r] = fma(fma(V[r], 2.0, s), 0.25, bias[r]);
+        x[r + 8] = fma(fma(V[r], -2.0, s), 0.25, bias[r + 8]);
+        x[r + 4] = fma(fma(V[r + 4], 2.0, t), 0.25, bias[r + 4]);
+        x[r + 12] = fma(fma(V[r + 4], -2.0, t), 0.25, bias[r + 12]);
     }
 }
 
@@ -185,20 +205,21 @@ __device__ __forceinline__ double t5_half_centred(uint32_t v) {
     return __hiloint2double(0x43300000, (int)v) - T5_HALF_BIAS;
 }
 
-__device__ __forceinline__ void t5_mds(uint64_t s[T5_STATE]) {
+// MDS of the state plus the round constants of round rnd.
+__device__ __forceinline__ void t5_mds(uint64_t s[T5_STATE], int rnd) {
     double dl[T5_STATE], dh[T5_STATE];
 #pragma unroll
     for (int c = 0; c < T5_STATE; c++) {
         dl[c] = t5_half_centred((uint32_t)s[c]);
         dh[c] = t5_half_centred((uint32_t)(s[c] >> 32));
     }
-    t5_mds_half(dl);
-    t5_mds_half(dh);
+    t5_mds_half(dl, c_t5_bias.lo + rnd * T5_STATE);
+    t5_mds_half(dh, c_t5_bias.hi + rnd * T5_STATE);
 #pragma unroll
     for (int r = 0; r < T5_STATE; r++) {
         const uint64_t lo = (uint64_t)__double_as_longlong(dl[r]) & 0xFFFFFFFFFFFFFull;
         const uint64_t hi = (uint64_t)__double_as_longlong(dh[r]) & 0xFFFFFFFFFFFFFull;
-        // lo + hi*2^32 as a 128-bit number (sh:sl) with sh < 2^21
+        // lo + hi*2^32 as a 128-bit number (sh:sl) with lo, hi < 2^52, sh < 2^20
         const uint64_t sl = lo + (hi << 32);
         const uint64_t sh = (hi >> 32) + (uint64_t)(sl < lo);
         const uint64_t v = sh * GL_EPS;  // < 2^53
@@ -231,9 +252,7 @@ __device__ __forceinline__ void t5_permutation(uint64_t s[T5_STATE], const uint3
 #pragma unroll
         for (int i = 0; i < 4; i++) s[i] = t5_split_lookup(s[i], lane_tbl);
         t5_pow7_layer(s);
-        t5_mds(s);
-#pragma unroll
-        for (int i = 0; i < T5_STATE; i++) s[i] = gl_add_pc(s[i], c_t5_rc[rnd * T5_STATE + i]);
+        t5_mds(s, rnd);  // and the round constants
     }
 }
 
@@ -243,9 +262,7 @@ __device__ __forceinline__ void t5_round(uint64_t s[T5_STATE], const uint32_t* l
 #pragma unroll
     for (int i = 0; i < 4; i++) s[i] = t5_split_lookup(s[i], lane_tbl);
     t5_pow7_layer(s);
-    t5_mds(s);
-#pragma unroll
-    for (int i = 0; i < T5_STATE; i++) s[i] = gl_add_pc(s[i], c_t5_rc[rnd * T5_STATE + i]);
+    t5_mds(s, rnd);
 }
 
 // Tip5::hash_pair / hash_10: rate = left || right, capacity = 1s.
