@@ -1,7 +1,7 @@
 // Host check of the Tip5 MDS half-product used by the GPU kernels
 // (t5_mds_half in tip5.cuh, compiled here for the CPU: the same IEEE-754 double
-// adds and fused multiply-adds as the FP64 pipe).  Each 32-bit half enters
-// centred through the kernels' own bias, and every output must equal the exact
+// adds and fused multiply-adds as the FP64 pipe).  Each 32-bit half v enters
+// as the kernels' biased double 2^52 + v, and every output must equal the exact
 // integer circulant product sum_c M[(r - c) mod 16] * v[c] plus the added
 // 32-bit value a[r] (a round constant's half in the kernels), plus 2^52.  Inputs:
 // all 2^16 patterns of {0, 2^32 - 1} (they reach the extreme value of every
@@ -17,10 +17,8 @@ static int check(const uint32_t v[16], const uint32_t a[16]) {
     static const long long M[16] = {TVMC_T5_MDS_FIRST_COLUMN};
     double x[16];
     for (int c = 0; c < 16; c++) {
-        const uint64_t b = 0x4330000000000000ull | v[c];  // the bits t5_half_centred starts from
-        double d;
-        memcpy(&d, &b, 8);
-        x[c] = d - T5_HALF_BIAS;
+        const uint64_t b = 0x4330000000000000ull | v[c];  // t5_half_biased(v[c])
+        memcpy(&x[c], &b, 8);
     }
     double bias[16];
     for (int r = 0; r < 16; r++) bias[r] = T5_MDS_BIAS + (double)a[r];
