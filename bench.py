@@ -325,10 +325,10 @@ def run_ours(args):
         hbm_peak, hbm_src = float(json.load(open(peaks_path))["hbm_gbs"]), "measured"
     int_peak = int_peak_tops(torch, dev)
     # DRAM bytes per k_hash_rows launch: one ncu capture of the 2^18-row x 379-column
-    # main-table launch (796.6 MB read + 12.2 MB written), scaled by rows
+    # main-table launch (795.3 MB read + 14.8 MB written), scaled by rows
     traffic, traffic_src = None, None
     if W_MAIN == 379:
-        traffic = (796.6e6 + 12.2e6) * L / (1 << 18)
+        traffic = (795.3e6 + 14.8e6) * L / (1 << 18)
         traffic_src = "ncu dram__bytes_read+write of a 2^18x379 launch, scaled by LDE rows (main table)"
 
     # e2e: pinned host traces through the public C ABI, roots read back
