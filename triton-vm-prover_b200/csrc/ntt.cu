@@ -307,14 +307,13 @@ __global__ void __launch_bounds__(NTT_THREADS) k_pass_b(const uint64_t* in, uint
 template <int LS>
 __global__ void __launch_bounds__(NTT_THREADS) k_lde_small(const uint64_t* trace, uint64_t tld, uint64_t* out,
                                                            uint64_t old, uint64_t cols, int lT, int le,
-                                                           const uint64_t* tw12_i, const uint64_t* tw12_f,
+                                                           const uint64_t* tw12_f,
                                                            const uint64_t* sc_lo, const uint64_t* sc_hi,
                                                            int hi_len, const uint64_t* add, int rm) {
     extern __shared__ uint64_t sm[];
     constexpr int n = 1 << LS;
     const int E = 1 << le;
-    uint64_t* twi = sm;                    // (unused: the inverse runs on the forward root)
-    uint64_t* twf = twi + n;
+    uint64_t* twf = sm;                    // forward root only (the inverse negates its input index)
     uint64_t* cf = twf + n;                // coefficients (natural order)
     uint64_t* s = cf + spad_words(n, lT);  // transposes
     load_tw<LS>(twf, tw12_f);
@@ -378,19 +377,17 @@ __global__ void __launch_bounds__(NTT_THREADS, L2 == 10 ? 2 : 1) k_lde_inv_a(con
 // Z_c[k2 + n2*q2].  Z holds E planes of N words per column: Z[(col*E + c)*N + .].
 template <int L1, bool RAND>
 __global__ void __launch_bounds__(NTT_THREADS) k_lde_mid(const uint64_t* Y, uint64_t yld, uint64_t* Z, int l2,
-                                                         int lT, int le, const uint64_t* tw12_i,
-                                                         const uint64_t* tw12_f, const uint64_t* wlo,
+                                                         int lT, int le, const uint64_t* tw12_f, const uint64_t* wlo,
                                                          const uint64_t* whi, const uint64_t* sc_lo,
                                                          const uint64_t* sc_hi, int hi_len, const uint64_t* add,
                                                          int rm) {
     extern __shared__ uint64_t sm[];
     constexpr int n1 = 1 << L1;
     const int E = 1 << le;
-    uint64_t* twi = sm;
-    uint64_t* twf = twi + n1;
+    uint64_t* twf = sm;  // forward root only (the inverse negates its input index)
     uint64_t* cf = twf + n1;                 // coefficients, natural k1 order
     uint64_t* s = cf + spad_words(n1, lT);   // transposes
-    load_tw<L1>(twf, tw12_f);  // the inverse also runs on the forward root (slot twi unused)
+    load_tw<L1>(twf, tw12_f);
     __syncthreads();
     const uint64_t col = blockIdx.y;
     const uint32_t k20 = blockIdx.x << lT;
@@ -434,7 +431,7 @@ __global__ void __launch_bounds__(NTT_THREADS) k_lde_mid(const uint64_t* Y, uint
 // second round goes through shared memory.
 template <int L1, bool RAND>
 __global__ void __launch_bounds__(128) k_lde_mid_reg(const uint64_t* Y, uint64_t yld, uint64_t* Z, int l2, int le,
-                                                     const uint64_t* tw12_i, const uint64_t* tw12_f,
+                                                     const uint64_t* tw12_f,
                                                      const uint64_t* wlo, const uint64_t* whi,
                                                      const uint64_t* sc_lo, const uint64_t* sc_hi, int hi_len,
                                                      const uint64_t* add, int rm) {
@@ -444,10 +441,9 @@ __global__ void __launch_bounds__(128) k_lde_mid_reg(const uint64_t* Y, uint64_t
     constexpr int lT = 7 - b2, T = 1 << lT;  // T * R2 = 128 threads
     constexpr int n1 = 1 << L1;
     extern __shared__ uint64_t sm[];
-    uint64_t* twi = sm;
-    uint64_t* twf = twi + n1;
+    uint64_t* twf = sm;  // forward root only (the inverse negates its input index)
     uint64_t* s = twf + n1;
-    load_tw<L1>(twf, tw12_f);  // the inverse also runs on the forward root (slot twi unused)
+    load_tw<L1>(twf, tw12_f);
     __syncthreads();
     const int E = 1 << le;
     const uint64_t col = blockIdx.y;
@@ -533,7 +529,7 @@ __global__ void __launch_bounds__(128) k_lde_mid_reg(const uint64_t* Y, uint64_t
 // instruction cache.  Thread (t, ln) owns line ln of every round.
 template <int L1, int MINB, bool RAND>
 __global__ void __launch_bounds__(128, MINB) k_lde_mid_sym(const uint64_t* Y, uint64_t yld, uint64_t* Z, int l2, int le,
-                                                     const uint64_t* tw12_i, const uint64_t* tw12_f,
+                                                     const uint64_t* tw12_f,
                                                      const uint64_t* wlo, const uint64_t* whi,
                                                      const uint64_t* sc_lo, const uint64_t* sc_hi, int hi_len,
                                                      const uint64_t* add, int rm) {
@@ -543,10 +539,9 @@ __global__ void __launch_bounds__(128, MINB) k_lde_mid_sym(const uint64_t* Y, ui
     constexpr int lT = 7 - B, T = 1 << lT;  // T * R = 128 threads
     constexpr int n1 = 1 << L1;
     extern __shared__ uint64_t sm[];
-    uint64_t* twi = sm;
-    uint64_t* twf = twi + n1;
+    uint64_t* twf = sm;  // forward root only (the inverse negates its input index)
     uint64_t* s = twf + n1;
-    load_tw<L1>(twf, tw12_f);  // the inverse also runs on the forward root (slot twi unused)
+    load_tw<L1>(twf, tw12_f);
     __syncthreads();
     const int E = 1 << le;
     const uint64_t col = blockIdx.y;
@@ -802,13 +797,13 @@ cudaError_t launch_lde(const LdePlan& pl, const uint64_t* trace, uint64_t tld, u
         }
         const int lT = choose_lT(l, 10);
         const int T = 1 << lT;
-        const size_t smem = words_bytes(2 * (size_t)(1u << l) + 2 * spad_words(1 << l, lT));
+        const size_t smem = words_bytes((size_t)(1u << l) + 2 * spad_words(1 << l, lT));
         return dispatch_ls(l, [&]<int LS>() -> cudaError_t {
             cudaError_t e = set_smem((const void*)k_lde_small<LS>, smem);
             if (e != cudaSuccess) return e;
             count_launch();
             k_lde_small<LS><<<(unsigned)((cols + T - 1) / T), NTT_THREADS, smem, st>>>(
-                trace, tld, out, old, cols, lT, le, pl.tw12_i, pl.tw12_f, pl.sc_lo, pl.sc_hi, hi_len, add, rm);
+                trace, tld, out, old, cols, lT, le, pl.tw12_f, pl.sc_lo, pl.sc_hi, hi_len, add, rm);
             return cudaGetLastError();
         });
     }
@@ -817,7 +812,7 @@ cudaError_t launch_lde(const LdePlan& pl, const uint64_t* trace, uint64_t tld, u
     const int lT1 = choose_lT(l2, 13);
     const size_t smem1 = words_bytes((1u << l2) + spad_words(1 << l2, lT1));
     const int lT2 = choose_lT(l1, 13);
-    const size_t smem2 = words_bytes(2 * (size_t)(1u << l1) + 2 * spad_words(1 << l1, lT2));
+    const size_t smem2 = words_bytes((size_t)(1u << l1) + 2 * spad_words(1 << l1, lT2));
     const int lT3 = clampi(13 - l2 - le, 0, 1);
     const size_t smem3 = words_bytes((1u << l2) + spad_words(1 << l2, lT3 + le));
     uint64_t* Y = scratch;
@@ -837,7 +832,7 @@ cudaError_t launch_lde(const LdePlan& pl, const uint64_t* trace, uint64_t tld, u
         e = dispatch_ls(l1, [&]<int L1>() -> cudaError_t {
             if constexpr (Plan<L1>::NR == 2 && Plan<L1>::b1 == Plan<L1>::b2) {
                 constexpr int lTr = 7 - Plan<L1>::b2;
-                const size_t smr = words_bytes(2 * (size_t)(1u << L1) + spad_words(1 << L1, lTr));
+                const size_t smr = words_bytes((size_t)(1u << L1) + spad_words(1 << L1, lTr));
                 // register budget: 2 resident CTAs (no spills) or 3 (a few spills); tuning knob
                 // (the randomized variant runs at 2 CTAs per SM)
                 auto kern = rm ? k_lde_mid_sym<L1, 2, true>
@@ -846,17 +841,17 @@ cudaError_t launch_lde(const LdePlan& pl, const uint64_t* trace, uint64_t tld, u
                 if (e2 != cudaSuccess) return e2;
                 count_launch();
                 kern<<<dim3((1u << l2) >> lTr, nc), 128, smr, st>>>(
-                    Y, N, Z, l2, le, pl.tw12_i, pl.tw12_f, pl.wn_f_lo, pl.wn_f_hi, pl.sc_lo, pl.sc_hi, hi_len,
+                    Y, N, Z, l2, le, pl.tw12_f, pl.wn_f_lo, pl.wn_f_hi, pl.sc_lo, pl.sc_hi, hi_len,
                     addc, rm);
             } else if constexpr (Plan<L1>::NR == 2) {
                 constexpr int lTr = 7 - Plan<L1>::b2;
-                const size_t smr = words_bytes(2 * (size_t)(1u << L1) + spad_words(1 << L1, lTr));
+                const size_t smr = words_bytes((size_t)(1u << L1) + spad_words(1 << L1, lTr));
                 auto kern = rm ? k_lde_mid_reg<L1, true> : k_lde_mid_reg<L1, false>;
                 cudaError_t e2 = set_smem((const void*)kern, smr);
                 if (e2 != cudaSuccess) return e2;
                 count_launch();
                 kern<<<dim3((1u << l2) >> lTr, nc), 128, smr, st>>>(
-                    Y, N, Z, l2, le, pl.tw12_i, pl.tw12_f, pl.wn_f_lo, pl.wn_f_hi, pl.sc_lo, pl.sc_hi, hi_len,
+                    Y, N, Z, l2, le, pl.tw12_f, pl.wn_f_lo, pl.wn_f_hi, pl.sc_lo, pl.sc_hi, hi_len,
                     addc, rm);
             } else {
                 auto kern = rm ? k_lde_mid<L1, true> : k_lde_mid<L1, false>;
@@ -864,7 +859,7 @@ cudaError_t launch_lde(const LdePlan& pl, const uint64_t* trace, uint64_t tld, u
                 if (e2 != cudaSuccess) return e2;
                 count_launch();
                 kern<<<dim3((1u << l2) >> lT2, nc), NTT_THREADS, smem2, st>>>(
-                    Y, N, Z, l2, lT2, le, pl.tw12_i, pl.tw12_f, pl.wn_f_lo, pl.wn_f_hi, pl.sc_lo, pl.sc_hi, hi_len,
+                    Y, N, Z, l2, lT2, le, pl.tw12_f, pl.wn_f_lo, pl.wn_f_hi, pl.sc_lo, pl.sc_hi, hi_len,
                     addc, rm);
             }
             return cudaGetLastError();
