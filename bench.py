@@ -10,10 +10,17 @@ no dataset for this path).
 Printed JSON (rank 0): `value` = committed LDE cells/s with the traces already
 in HBM (device-timed with CUDA events); `e2e` = the same through the public
 C ABI from pinned host buffers (upload inside the timed region, roots read
-back); `roofline` = the dominant kernel (Tip5 row hash + tree) against the
-measured int32 issue peak; `roofline_lde` = the LDE kernels against HBM;
-`cpu_baseline` = the reference's own CPU code (oracle/_ref) on a bounded
-sample on this host's cores.
+back); `roofline` = the dominant kernel (Tip5 row hash + tree) against the SM
+instruction-issue limit (SMs x 4 schedulers x 32 lanes x the SM clock sampled
+during the timed region); `roofline_lde` = the LDE kernels against HBM;
+`roofline_commit` = the whole step against the slower of its HBM bytes at the
+measured copy bandwidth and its integer ops (Tip5 + NTT cost model) at the
+issue limit; `cpu_baseline` = the reference's own CPU code (oracle/_ref) on a
+bounded sample on this host's cores, extrapolated to the workload.
+
+`--impl reference` times the reference's own CPU code (oracle/_ref, OpenMP on
+every host core) on one full step of the same workload, plus the as-shipped
+serial figure (one thread) on the 2^10 x 379 commit.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -53,10 +60,44 @@ METRIC = "committed LDE cells/s"
 # Tip5 integer-op cost model (32-bit ops): Goldilocks mul 16, add 4; one
 # permutation = 5 x (12 x^7 @ 4 muls + 4 split-and-lookup @ 48 + MDS @ 640 + 16 RC adds @ 4).
 OPS_PER_PERM = 5 * (12 * 4 * 16 + 4 * 48 + 640 + 16 * 4)
+# NTT cost model: 24 int32 ops per butterfly or scale.
+OPS_PER_NTT_MUL = 24
+# Instruction issue of one SM per clock: 4 schedulers x 32 lanes.
+ISSUE_LANES_PER_SM = 4 * 32
 
 
 def perms_per_table(L: int, width: int) -> int:
     return L * (width // 10 + 1) + (L - 1)
+
+
+def ntt_ops_per_table(n: int, width: int, expansion: int = EXPANSION) -> int:
+    """Cost-model int32 ops of one table's LDE: per column an n-point inverse
+    NTT, n coset scales and an (expansion*n)-point forward NTT."""
+    L = expansion * n
+    ln, lL = n.bit_length() - 1, L.bit_length() - 1
+    return width * ((n // 2) * ln + n + (L // 2) * lL) * OPS_PER_NTT_MUL
+
+
+def bytes_per_table(n: int, width: int, expansion: int = EXPANSION) -> int:
+    """Algorithmic bytes of one commit: trace read, LDE written, leaf digests,
+    internal nodes."""
+    L = expansion * n
+    return 8 * n * width + 8 * L * width + 40 * L + 40 * (L - 1)
+
+
+def issue_limit_tops(sms: int, sm_mhz: float) -> float:
+    """Thread-instructions per second the SMs can issue (T/s)."""
+    return sms * ISSUE_LANES_PER_SM * sm_mhz * 1e6 / 1e12
+
+
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 def max_over_ranks(x: float, device=None) -> float:
@@ -131,22 +172,6 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-def int_peak_tops(torch, dev) -> float:
-    """Measured int32 issue throughput (Top/s) of an independent IADD3/LOP3/IMAD
-    mix, from this repo's own probe kernel (libtvmc: tvmc_int_peak_probe)."""
-    import tvmc
-    L = tvmc.lib()
-    if not hasattr(L, "tvmc_int_peak_probe"):
-        return float("nan")
-    import ctypes
-    L.tvmc_int_peak_probe.restype = ctypes.c_double
-    L.tvmc_int_peak_probe.argtypes = [ctypes.c_void_p]
-    best = 0.0
-    for _ in range(3):
-        best = max(best, L.tvmc_int_peak_probe(torch.cuda.current_stream(dev).cuda_stream))
-    return best / 1e12
-
-
 def random_trace(torch, width, n, seed, dev):
     g = torch.Generator(device=dev).manual_seed(seed)
     hi = torch.randint(0, 2**32, (width, n), dtype=torch.int64, device=dev, generator=g)
@@ -197,35 +222,95 @@ def cpu_reference_sample(log_n: int, threads: int | None = None):
     cells = L * (W_MAIN + W_AUX)
     sample = (f"reference CPU code (oracle/_ref, OpenMP): LDE of {ncol} columns 2^{log_n}->2^{log_n + 2}, "
               f"Tip5 hash of {rows} rows x 379 and x 264, Merkle of {nl} leaves; extrapolated linearly to "
-              f"2^{log_n + 2} rows x (379 + 264) columns")
+              f"2^{log_n + 2} rows x (379 + 264) columns (an estimate; --impl reference times a full step)")
     detail = {"lde_s": lde_total, "hash_s": hash_total, "merkle_s": merkle_total, "sample_s": t_lde + t_hm + t_ha +
               t_m, "est_commit_s": total}
     del lde
     return cells / total, cores, sample, detail
 
 
+def host_mem_available() -> int:
+    try:
+        for line in open("/proc/meminfo"):
+            if line.startswith("MemAvailable:"):
+                return int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    return 0
+
+
 def run_reference(args):
+    """The reference's own CPU path (oracle/_ref: LDE::extend_column per
+    column, Tip5::hash_varlen per row, MerkleTree) on every host core.  The
+    timed step is one full commit of the workload (main and aux tables, two
+    trees); with W >= 1 warm-up steps of the 2^10 x 379 commit first.  A full
+    CPU step takes minutes, so `--steps` is capped by --ref-max-seconds: the
+    line reports the steps actually timed.  The sample extrapolation
+    (cpu_reference_sample) runs first as a cross-check and as the fallback when
+    the host lacks the memory or time for a full step."""
     ws, rank, _ = dist_info()
     if rank != 0:
         return
-    vals = []
-    cores, sample = None, None
-    for i in range(args.warmup + args.steps):
-        v, cores, sample, _ = cpu_reference_sample(args.log_n)
-        if i >= args.warmup:
-            vals.append(v)
-    value = statistics.median(vals)
-    L = EXPANSION << args.log_n
+    from oracle import RefLib
+    r = RefLib()
+    cores = r.max_threads()
+    n = 1 << args.log_n
+    L = EXPANSION * n
     cells = L * (W_MAIN + W_AUX)
-    line = {"metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * cells / value, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "u64 (Goldilocks)", "data": "synthetic",
-            "impl": "reference",
-            "config": {"workload": f"main 2^{args.log_n}x{W_MAIN} + aux 2^{args.log_n}x{W_AUX} limbs, x4 LDE, Tip5 rows, "
-                                   "Merkle", "trace_len": 1 << args.log_n, "widths": [W_MAIN, W_AUX],
-                       "expansion": EXPANSION, "parallelism": "cpu"},
+    rng = np.random.default_rng(0x7E5EED01)
+    small = rng.integers(0, P, (W_MAIN, 1 << 10), dtype=np.uint64)
+    for _ in range(args.warmup):
+        r.commit(small, EXPANSION, OFFSET)
+    # as-shipped serial figure: the 2^10 x 379 commit on one thread
+    r.set_threads(1)
+    t0 = time.perf_counter()
+    r.commit(small, EXPANSION, OFFSET)
+    serial_s = time.perf_counter() - t0
+    r.set_threads(cores)
+    est_v, _, est_sample, est_detail = cpu_reference_sample(args.log_n)
+    est_s = est_detail["est_commit_s"]
+    need = 8 * n * (W_MAIN + W_AUX) + 8 * L * max(W_MAIN, W_AUX) + 2 * (8 << 30)
+    full = host_mem_available() >= need and est_s <= args.ref_max_seconds
+    times = []
+    if full:
+        main_t = rng.integers(0, P, (W_MAIN, n), dtype=np.uint64)
+        aux_t = rng.integers(0, P, (W_AUX, n), dtype=np.uint64)
+        buf = np.empty(L * max(W_MAIN, W_AUX), dtype=np.uint64)
+        budget = args.ref_max_seconds
+        spent = 0.0
+        while len(times) < max(1, args.steps) and spent + (times[-1] if times else est_s) <= budget:
+            t0 = time.perf_counter()
+            r.commit(main_t, EXPANSION, OFFSET, lde_buf=buf)
+            r.commit(aux_t, EXPANSION, OFFSET, lde_buf=buf)
+            times.append(time.perf_counter() - t0)
+            spent += times[-1]
+        del buf, main_t, aux_t
+    if times:
+        step_s = statistics.median(times)
+        value = cells / step_s
+        sample = (f"full steps timed: main 2^{args.log_n}x{W_MAIN} + aux 2^{args.log_n}x{W_AUX} limbs committed "
+                  f"by the reference's CPU code (oracle/_ref, OpenMP over columns and rows, {cores} threads)")
+    else:
+        step_s = est_s
+        value = est_v
+        sample = est_sample + (" [fallback: host memory or the time cap does not allow a full step]")
+    line = {"metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": args.gpus, "steps": len(times) or 0,
+            "steps_requested": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * step_s,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64 (Goldilocks)",
+            "data": "synthetic uniform field elements", "impl": "reference",
+            "timed": "full step" if times else "extrapolated sample",
+            "config": {"workload": f"main 2^{args.log_n}x{W_MAIN} + aux 2^{args.log_n}x{W_AUX} limbs, x4 LDE (offset 7), "
+                                   "Tip5 row hash, Merkle (two trees)", "trace_len": n, "lde_len": L,
+                       "widths": [W_MAIN, W_AUX], "expansion": EXPANSION, "cells_per_step": cells,
+                       "parallelism": "cpu"},
             "cpu_baseline": {"value": value, "unit": "cells/s", "cores": cores, "kind": "reference",
-                             "sample": sample},
+                             "sample": sample, "cpu_model": cpu_model(),
+                             "step_seconds": times,
+                             "sample_estimate": {"value": est_v, "est_step_s": est_s, "sample": est_sample},
+                             "serial_2p10x379": {"seconds": serial_s, "cells_per_s": (4 << 10) * W_MAIN / serial_s,
+                                                 "threads": 1,
+                                                 "what": "as-shipped serial path: LDE::extend_column per column, "
+                                                         "Tip5::hash_varlen per row, MerkleTree, one thread"}},
             "e2e": {"value": value, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -323,7 +408,23 @@ def run_ours(args):
     hbm_peak, hbm_src = 6650.0, "fallback"
     if os.path.exists(peaks_path):
         hbm_peak, hbm_src = float(json.load(open(peaks_path))["hbm_gbs"]), "measured"
-    int_peak = int_peak_tops(torch, dev)
+    clocks = clk.summary()
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    sm_mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 1965.0
+    int_peak = issue_limit_tops(sms, sm_mhz)
+    # whole step: the slower of its HBM bytes and its integer work
+    step_bytes = sum(bytes_per_table(n, w) for w in (W_MAIN, W_AUX))
+    step_int_ops = sum(perms_per_table(L, w) * OPS_PER_PERM + ntt_ops_per_table(n, w) for w in (W_MAIN, W_AUX))
+    hbm_ms = step_bytes / (hbm_peak * 1e9) * 1e3
+    int_ms = step_int_ops / (int_peak * 1e12) * 1e3
+    ms_step = t_max / args.steps
+    roof_commit = {"bound": "int32" if int_ms >= hbm_ms else "hbm", "roofline_ms_per_step": max(hbm_ms, int_ms),
+                   "ms_per_step": ms_step, "frac": max(hbm_ms, int_ms) / ms_step,
+                   "hbm_ms": hbm_ms, "int_ms": int_ms, "bytes_per_step": step_bytes,
+                   "int_ops_per_step": step_int_ops, "hbm_peak_gbs": hbm_peak, "hbm_peak_source": hbm_src,
+                   "int_peak_tops": int_peak,
+                   "cost_model": f"Tip5 {OPS_PER_PERM} int32 ops per permutation; NTT {OPS_PER_NTT_MUL} per "
+                                 "butterfly or scale; bytes 8NW + 32NW + 40*4N + 40*(4N-1) per table"}
     # DRAM bytes per k_hash_rows launch: one ncu capture of the 2^18-row x 379-column
     # main-table launch (795.3 MB read + 14.8 MB written), scaled by rows
     traffic, traffic_src = None, None
@@ -382,7 +483,7 @@ def run_ours(args):
     if rank == 0 and ws == 1 and not args.skip_cpu:
         v, cores, sample, detail = cpu_reference_sample(args.log_n)
         cpu = {"value": v, "unit": "cells/s", "cores": cores, "kind": "reference", "sample": sample,
-               "est_commit_s": detail["est_commit_s"]}
+               "est_commit_s": detail["est_commit_s"], "extrapolated": True, "cpu_model": cpu_model()}
 
     if rank == 0:
         line = {
@@ -397,13 +498,16 @@ def run_ours(args):
                        "tuning": tuned.get("knobs", {}), "tuning_s": tuned.get("seconds", {}),
                        "streams": args.streams,
                        "parallelism": "replicas" if ws > 1 else "1 gpu"},
-            "roofline": {"bound": "int32", "kernel": "k_hash_rows + k_merkle_up (Tip5)",
+            "roofline": {"bound": "int32", "kernel": "k_hash_rows + k_merkle_level + k_merkle_up (Tip5)",
                          "achieved": achieved_int, "peak": int_peak, "unit": "Top/s",
-                         "frac": achieved_int / int_peak if int_peak == int_peak else None,
-                         "peak_source": "measured int32 issue probe (tvmc_int_peak_probe)",
-                         "traffic": traffic, "traffic_source": traffic_src, "cost_model": f"{OPS_PER_PERM} int32 ops per Tip5 permutation",
+                         "frac": achieved_int / int_peak,
+                         "peak_source": f"SM issue limit: {sms} SMs x {ISSUE_LANES_PER_SM} lanes x {sm_mhz:.0f} MHz "
+                                        "(median SM clock sampled in the timed region)",
+                         "traffic": traffic, "traffic_source": traffic_src,
+                         "cost_model": f"{OPS_PER_PERM} int32 ops per Tip5 permutation",
                          "ms_per_step": sum(hash_ms) / args.steps,
                          "ms_per_table_min_max": [min(hash_ms), max(hash_ms)]},
+            "roofline_commit": roof_commit,
             "roofline_lde": {"bound": "hbm", "achieved": achieved_hbm, "peak": hbm_peak, "unit": "GB/s",
                              "frac": achieved_hbm / hbm_peak, "peak_source": hbm_src,
                              "bytes": "8*N*W read + 8*4N*W written per table",
@@ -411,7 +515,7 @@ def run_ours(args):
                              "ms_per_table_min_max": [min(lde_ms), max(lde_ms)]},
             "e2e": e2e,
             "cpu_baseline": cpu,
-            "clocks": clk.summary(),
+            "clocks": clocks,
             "gpu_launches": launches,
         }
         print(json.dumps(line), flush=True)
@@ -658,6 +762,8 @@ def main():
     ap.add_argument("--workload", choices=["commit", "batch", "frugal", "serving"], default="commit")
     ap.add_argument("--streams", type=int, default=1,
                     help="commit, device-timed part: main and aux on 1 or 2 streams (e2e always uses 2)")
+    ap.add_argument("--ref-max-seconds", type=float, default=600.0,
+                    help="reference arm: time budget for its full CPU steps")
     ap.add_argument("--requests", type=int, default=48, help="serving: requests per rate")
     ap.add_argument("--serve-streams", type=int, default=4)
     ap.add_argument("--serve-max-log-n", type=int, default=20)

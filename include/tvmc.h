@@ -207,7 +207,11 @@ typedef struct tvmc_commitment tvmc_commitment;
  *                         spills) or 3 (a few spills); default 2
  *   "hash_unfused_tree"   1: build every Merkle level in the tree kernel instead of the lowest
  *                         eight inside the row-hash CTAs; default 0
- * Unknown keys return TVMC_ERR_INVALID. */
+ *   "fail_alloc_after"    fault injection for tests: k > 0 makes the k-th device allocation the
+ *                         library requests from now on fail as out-of-memory (once, on the host,
+ *                         without reaching the driver); 0 disables
+ * Unknown keys return TVMC_ERR_INVALID.  tvmc_get_tuning also reads "pool_used_bytes": the bytes
+ * currently allocated from the current device's stream-ordered pool (a leak check). */
 int tvmc_set_tuning(const char* key, long long value);
 /* The library keeps its LDE/NTT scratch, upload staging and the LDE of
  * TVMC_DISCARD_LDE commitments per (device, stream) once used, and the device's
@@ -397,11 +401,6 @@ int tvmc_server_destroy(tvmc_server* s);
 int tvmc_commitment_phase_ms(tvmc_commitment* c, float* ms3);
 /* Total kernels launched by this library so far (all threads and devices). */
 unsigned long long tvmc_launch_count(void);
-/* Measured 32-bit integer instruction issue rate of the current device
- * (thread-instructions per second, an even IMAD/ALU mix); the denominator of
- * the Tip5 roofline.  Synchronizes `stream`; returns < 0 on failure.
- * No reference counterpart (measurement utility). */
-double tvmc_int_peak_probe(void* stream);
 
 #ifdef __cplusplus
 }

@@ -16,6 +16,10 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 P = 0xFFFFFFFF00000001
+# The reference source tree: environment variable REF (the Makefiles under
+# oracle/, tests/cpp/ and triton-vm-prover_b200/cpp/ read the same variable).
+# Only present on the development host; the GPU host uses the prebuilt files.
+REF_DIR = os.environ.get("REF", "/root/reference")
 
 _u64p = ctypes.POINTER(ctypes.c_uint64)
 _szp = ctypes.POINTER(ctypes.c_size_t)
@@ -29,8 +33,8 @@ def build(ref: bool = True) -> None:
     """Compile liboracle.so (always) and _ref/libtvm_ref.so (when the
     reference sources are present)."""
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
-    if ref and os.path.isdir("/root/reference/src"):
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+    if ref and os.path.isdir(os.path.join(REF_DIR, "src")):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REF_DIR}"], check=True)
 
 
 class Oracle:
@@ -52,6 +56,7 @@ class Oracle:
         L.tvmo_ntt_inverse.argtypes = [_u64p, ctypes.c_size_t]
         L.tvmo_lde_table.argtypes = [_u64p, ctypes.c_size_t, ctypes.c_size_t, _u64p, ctypes.c_size_t,
                                      ctypes.c_uint64]
+        L.tvmo_evaluate_on_coset.argtypes = [_u64p, ctypes.c_size_t, _u64p, ctypes.c_size_t, ctypes.c_uint64]
         L.tvmo_tip5_permutation.argtypes = [_u64p]
         L.tvmo_hash_varlen.argtypes = [_u64p, ctypes.c_size_t, _u64p]
         L.tvmo_hash_10.argtypes = [_u64p, _u64p]
@@ -81,6 +86,15 @@ class Oracle:
         if fn(_ptr(a), a.size) != 0:
             raise ValueError("NTT size must be a power of 2")
         return a
+
+    def evaluate_on_coset(self, coeffs, domain_len: int, offset: int) -> np.ndarray:
+        """NTT::evaluate_on_coset of one coefficient vector (any length)."""
+        c = np.ascontiguousarray(coeffs, dtype=np.uint64)
+        out = np.empty(domain_len, dtype=np.uint64)
+        cc = c if c.size else np.zeros(1, np.uint64)
+        if self.L.tvmo_evaluate_on_coset(_ptr(cc), c.size, _ptr(out), domain_len, offset) != 0:
+            raise ValueError("NTT size must be a power of 2")
+        return out
 
     def lde(self, trace_cm: np.ndarray, expansion: int = 4, offset: int = 7) -> np.ndarray:
         """Column-major (width, n) -> column-major (width, expansion*n)."""
@@ -197,6 +211,7 @@ class RefLib:
         L.tvmr_ntt.argtypes = [_u64p, ctypes.c_size_t, ctypes.c_int]
         L.tvmr_lde_table.argtypes = [_u64p, ctypes.c_size_t, ctypes.c_size_t, _u64p, ctypes.c_size_t,
                                      ctypes.c_uint64]
+        L.tvmr_evaluate_on_coset.argtypes = [_u64p, ctypes.c_size_t, _u64p, ctypes.c_size_t, ctypes.c_uint64]
         L.tvmr_hash_rows.argtypes = [_u64p, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t,
                                      ctypes.c_size_t, _u64p]
         L.tvmr_merkle.argtypes = [_u64p, ctypes.c_size_t, _u64p]
@@ -245,6 +260,13 @@ class RefLib:
         a = np.ascontiguousarray(a, dtype=np.uint64).copy()
         self.L.tvmr_ntt(_ptr(a), a.size, int(inverse))
         return a
+
+    def evaluate_on_coset(self, coeffs, domain_len, offset):
+        c = np.ascontiguousarray(coeffs, dtype=np.uint64)
+        out = np.empty(domain_len, dtype=np.uint64)
+        cc = c if c.size else np.zeros(1, np.uint64)
+        self.L.tvmr_evaluate_on_coset(_ptr(cc), c.size, _ptr(out), domain_len, offset)
+        return out
 
     def lde(self, trace_cm, expansion=4, offset=7):
         t = np.ascontiguousarray(trace_cm, dtype=np.uint64)
@@ -323,10 +345,16 @@ class RefLib:
             raise IndexError("Leaf index out of range")
         return out[:k]
 
-    def commit(self, trace_cm, expansion=4, offset=7):
+    def commit(self, trace_cm, expansion=4, offset=7, lde_buf=None):
+        """The reference's CPU commit of one column-major table; returns
+        (LDE, root).  lde_buf: an optional flat uint64 buffer of at least
+        width * n * expansion words to hold the LDE (reused across calls)."""
         t = np.ascontiguousarray(trace_cm, dtype=np.uint64)
         w, n = t.shape
-        lde = np.empty((w, n * expansion), dtype=np.uint64)
+        if lde_buf is None:
+            lde = np.empty((w, n * expansion), dtype=np.uint64)
+        else:
+            lde = lde_buf[: w * n * expansion].reshape(w, n * expansion)
         root = np.zeros(5, dtype=np.uint64)
         if self.L.tvmr_commit(_ptr(t), n, w, n * expansion, offset, _ptr(lde), _ptr(root)) != 0:
             raise ValueError("commit failed")

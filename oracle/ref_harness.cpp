@@ -76,6 +76,14 @@ void tvmr_ntt(uint64_t* a, size_t n, int inverse) {
     for (size_t i = 0; i < n; i++) a[i] = v[i].value();
 }
 
+// NTT::evaluate_on_coset (src/ntt/ntt.cpp:94-117) of one coefficient vector.
+void tvmr_evaluate_on_coset(const uint64_t* coeffs, size_t n, uint64_t* out, size_t L, uint64_t offset) {
+    std::vector<BFieldElement> c(n);
+    for (size_t i = 0; i < n; i++) c[i] = BFieldElement(coeffs[i]);
+    std::vector<BFieldElement> e = NTT::evaluate_on_coset(c, L, BFieldElement(offset));
+    for (size_t j = 0; j < L; j++) out[j] = e[j].value();
+}
+
 // Column-major LDE of `width` columns: trace[c*n + r] -> lde[c*L + r].
 void tvmr_lde_table(const uint64_t* trace, size_t n, size_t width, uint64_t* lde, size_t L,
                     uint64_t offset) {

@@ -129,6 +129,18 @@ def test_oracle_matches_reference_build(oracle):
     assert (oracle.merkle(leaves)[1:] == r.merkle(leaves)[1:]).all()
 
 
+@pytest.mark.skipif(not _ref_available(), reason="reference build oracle/_ref not present")
+def test_oracle_evaluate_on_coset_matches_reference_build(oracle):
+    """NTT::evaluate_on_coset: zero-extension (n < L), equal sizes and the
+    reference's truncation of coefficients beyond the domain (n > L)."""
+    from oracle import RefLib
+    r = RefLib()
+    for n, L, off in ((0, 8, 7), (1, 1, 7), (5, 16, 7), (64, 64, 3), (100, 32, 7), (1 << 10, 1 << 13, 7),
+                      (1 << 12, 1 << 12, 0xFFFFFFFF00000000)):
+        c = rand_u64(n + L, n)
+        assert (oracle.evaluate_on_coset(c, L, off) == r.evaluate_on_coset(c, L, off)).all(), (n, L)
+
+
 def test_lde_randomized_golden(oracle):
     """The oracle's randomized LDE equals the reference's RandomizedLDE outputs."""
     g = golden("lde_randomized.npz")

@@ -8,14 +8,16 @@ import subprocess
 import pytest
 
 from conftest import ROOT
+from oracle import REF_DIR
 
-REF_INCLUDE = "/root/reference/include"
+REF_INCLUDE = os.path.join(REF_DIR, "include")
 BIN = os.path.join(ROOT, "tests", "cpp", "_bin", "shim_selftest")
 
 
 @pytest.mark.skipif(not os.path.isdir(REF_INCLUDE), reason="reference headers not present")
 def test_shim_compiles_against_reference_headers():
-    r = subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "triton-vm-prover_b200", "cpp"), "check"],
+    r = subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "triton-vm-prover_b200", "cpp"), "check",
+                        f"REF={REF_DIR}"],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr[-4000:]
 

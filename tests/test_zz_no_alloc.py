@@ -46,6 +46,25 @@ def test_noalloc_lde_equals_allocating_lde_on_two_consecutive_calls(tv):
     assert (new == ref).all()
 
 
+@pytest.mark.parametrize("width,log_n,expansion,offset", [
+    (7, 6, 4, 7),    # small-LDE kernel (whole columns per CTA)
+    (2, 0, 2, 7),    # one-row traces
+    (1, 16, 1, 7),   # expansion 1
+    (1, 18, 16, 5),  # expansion 16: the largest coset-scale tables
+])
+def test_noalloc_lde_equals_allocating_lde_across_kernel_paths(tv, width, log_n, expansion, offset):
+    ref, new = _both(tv, rand_u64(200 + log_n, (width, 1 << log_n)), expansion, offset)
+    assert (new == ref).all()
+
+
+def test_noalloc_lde_repeated_and_changed_parameters(tv):
+    # the same size and offset twice (the second call reuses the tables already
+    # in the array), then a different offset at the same size, then back again
+    for seed, offset in ((300, 7), (301, 7), (302, 3), (303, 7)):
+        ref, new = _both(tv, rand_u64(seed, (3, 1 << 12)), 4, offset)
+        assert (new == ref).all(), offset
+
+
 def test_noalloc_lde_refuses_sizes_beyond_the_static_array(tv):
     lib = tv.lib()
     d = dev_empty(8)
@@ -53,3 +72,6 @@ def test_noalloc_lde_refuses_sizes_beyond_the_static_array(tv):
     rc = lib.tvmc_lde_batch_noalloc_gpu(d.data_ptr(), 1, 1 << 21, d.data_ptr(), 1 << 23, 1, 7, None)
     assert rc == tv.ERR_UNSUPPORTED
     assert b"static scratch" in lib.tvmc_last_error()
+    # the size rules are the allocating entry point's own
+    rc = lib.tvmc_lde_batch_noalloc_gpu(d.data_ptr(), 1, 12, d.data_ptr(), 48, 1, 7, None)
+    assert rc == tv.ERR_INVALID and b"power of 2" in lib.tvmc_last_error()

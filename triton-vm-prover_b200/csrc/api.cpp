@@ -55,6 +55,34 @@ int cuda_fail(cudaError_t e, const char* where) {
         if (e_ != cudaSuccess) return cuda_fail(e_, #expr); \
     } while (0)
 
+// Allocation-failure injection (tuning key "fail_alloc_after" = k > 0): the
+// k-th device allocation this library requests from then on fails with
+// cudaErrorMemoryAllocation without reaching the driver, once.  A host-side
+// fault for tests of the out-of-memory paths (the counterpart of the
+// reference's pre-flight check_gpu_memory, src/gpu/gpu_stark.cu:1588-1730);
+// the GPU itself sees nothing.
+std::atomic<long long> g_fail_alloc_after{0};
+
+bool injected_alloc_failure() {
+    long long k = g_fail_alloc_after.load();
+    while (k > 0) {
+        if (g_fail_alloc_after.compare_exchange_weak(k, k - 1)) return k == 1;
+    }
+    return false;
+}
+
+// Every device allocation of this file goes through these two.
+template <class T>
+cudaError_t dev_malloc(T** p, size_t bytes) {
+    if (injected_alloc_failure()) return cudaErrorMemoryAllocation;
+    return cudaMalloc((void**)p, bytes);
+}
+template <class T>
+cudaError_t dev_malloc_async(T** p, size_t bytes, cudaStream_t st) {
+    if (injected_alloc_failure()) return cudaErrorMemoryAllocation;
+    return cudaMallocAsync((void**)p, bytes, st);
+}
+
 bool is_pow2(size_t n) { return n != 0 && (n & (n - 1)) == 0; }
 int log2u(size_t n) {
     int k = 0;
@@ -90,7 +118,7 @@ std::mutex g_mu;
 std::map<int, DevTables> g_dev;
 
 cudaError_t upload(const std::vector<uint64_t>& h, uint64_t** d) {
-    cudaError_t e = cudaMalloc(d, h.size() * 8);
+    cudaError_t e = dev_malloc(d, h.size() * 8);
     if (e != cudaSuccess) return e;
     return cudaMemcpy(*d, h.data(), h.size() * 8, cudaMemcpyHostToDevice);
 }
@@ -224,7 +252,7 @@ int build_rand_add(const uint64_t* d_r, size_t R, size_t width, int logn, int le
     if (R == 0 || width == 0) return TVMC_OK;
     const int rm = rand_rows(logn, R);
     const size_t N = size_t(1) << logn, L = N << le;
-    CK(cudaMallocAsync((void**)buf, width * ((size_t)rm << le) * 8, st));
+    CK(dev_malloc_async((void**)buf, width * ((size_t)rm << le) * 8, st));
     const uint64_t tc = t % P, oc = o % P;
     const uint64_t qlen = truncate ? std::min<uint64_t>(N + R, L) : N + R;
     cudaError_t e = launch_rand_addend(d_r, R, width, logn, le, tc, hpow(tc, N), hpow(oc, N), root_of_unity(le),
@@ -273,7 +301,7 @@ int stream_scratch(cudaStream_t st, size_t words, uint64_t** out, int kind = 0, 
         if (slot.p) cudaFreeAsync(slot.p, st);  // ordered after the work that used it
         if (slot.last_use) cudaEventDestroy(slot.last_use);
         slot = ScratchSlot{};
-        CK(cudaMallocAsync((void**)&slot.p, words * 8, st));
+        CK(dev_malloc_async((void**)&slot.p, words * 8, st));
         slot.words = words;
         if (grown) *grown = true;
     }
@@ -413,18 +441,6 @@ int upload_lde_pipelined(const LdePlan& pl, const uint64_t* h_trace, size_t n, s
     return TVMC_OK;
 }
 
-int check_lde_sizes(size_t trace_len, size_t extended_len, int* logn, int* le) {
-    if (!is_pow2(trace_len)) return fail(TVMC_ERR_INVALID, "trace length %zu is not a power of 2", trace_len);
-    if (!is_pow2(extended_len) || extended_len < trace_len)
-        return fail(TVMC_ERR_INVALID, "extended length %zu is not a power of 2 >= trace length", extended_len);
-    *logn = log2u(trace_len);
-    *le = log2u(extended_len) - *logn;
-    if (*logn > MAX_LOG_LDE_TRACE)
-        return fail(TVMC_ERR_UNSUPPORTED, "LDE trace length 2^%d exceeds 2^%d", *logn, MAX_LOG_LDE_TRACE);
-    if (*le > 4) return fail(TVMC_ERR_UNSUPPORTED, "expansion factor 2^%d exceeds 16", *le);
-    return TVMC_OK;
-}
-
 int ntt_impl(uint64_t* d, size_t n, size_t cols, int inverse, cudaStream_t st) {
     if (!is_pow2(n)) return fail(TVMC_ERR_INVALID, "NTT size must be a power of 2 (got %zu)", n);
     int l = log2u(n);
@@ -446,7 +462,7 @@ struct DBuf {
     ~DBuf() {
         if (p) cudaFree(p);
     }
-    cudaError_t alloc(size_t words) { return cudaMalloc((void**)&p, words ? words * 8 : 8); }
+    cudaError_t alloc(size_t words) { return dev_malloc((void**)&p, words ? words * 8 : 8); }
 };
 
 // Per-thread, per-device device buffer reused by the host-buffer entry points,
@@ -479,7 +495,7 @@ int host_buf(size_t words, HostBuf* hb) {
         if (b.first) cudaFree(b.first);
         b = {nullptr, 0};
         const size_t cap = std::max(words, size_t(1) << 16);
-        CK(cudaMalloc((void**)&b.first, cap * 8));
+        CK(dev_malloc((void**)&b.first, cap * 8));
         b.second = cap;
     }
     hb->p = b.first;
@@ -521,12 +537,12 @@ int commit_frugal(const LdePlan& pl, const uint64_t* trace, bool dev, bool rm, s
     uint64_t *up = nullptr, *cm = nullptr, *cap = nullptr, *stripe = nullptr, *scratch = nullptr;
     cudaError_t e = cudaSuccess;
     if (width && !dev) {
-        e = cudaMallocAsync((void**)&up, NW * 8, st);
+        e = dev_malloc_async((void**)&up, NW * 8, st);
         if (e == cudaSuccess) e = cudaMemcpyAsync(up, trace, NW * 8, cudaMemcpyHostToDevice, st);
         src = up;
     }
     if (e == cudaSuccess && width && rm) {
-        e = cudaMallocAsync((void**)&cm, NW * 8, st);
+        e = dev_malloc_async((void**)&cm, NW * 8, st);
         if (e == cudaSuccess) e = launch_transpose(src, width, cm, n, n, width, st);
         src = cm;
     }
@@ -537,8 +553,8 @@ int commit_frugal(const LdePlan& pl, const uint64_t* trace, bool dev, bool rm, s
     sc = std::max<size_t>(10, sc / 10 * 10);
     const size_t stripe_cols = std::min(sc, std::max<size_t>(width, 1));
     const size_t chunk = std::min(lde_chunk_cols(pl.logn, pl.log_exp, stripe_cols), stripe_cols);
-    if (e == cudaSuccess) e = cudaMallocAsync((void**)&cap, 6 * L * 8, st);
-    if (e == cudaSuccess && width) e = cudaMallocAsync((void**)&stripe, stripe_cols * L * 8, st);
+    if (e == cudaSuccess) e = dev_malloc_async((void**)&cap, 6 * L * 8, st);
+    if (e == cudaSuccess && width) e = dev_malloc_async((void**)&stripe, stripe_cols * L * 8, st);
     if (e == cudaSuccess && stream_scratch(st, lde_scratch_words(pl.logn, pl.log_exp, chunk), &scratch))
         e = cudaErrorMemoryAllocation;
     size_t c0 = 0;
@@ -583,6 +599,18 @@ int auth_structure_nodes(size_t n, const size_t* leaf_idx, size_t count, std::ve
 }
 
 }  // namespace
+
+int tvmc::check_lde_sizes(size_t trace_len, size_t extended_len, int* logn, int* le) {
+    if (!is_pow2(trace_len)) return fail(TVMC_ERR_INVALID, "trace length %zu is not a power of 2", trace_len);
+    if (!is_pow2(extended_len) || extended_len < trace_len)
+        return fail(TVMC_ERR_INVALID, "extended length %zu is not a power of 2 >= trace length", extended_len);
+    *logn = log2u(trace_len);
+    *le = log2u(extended_len) - *logn;
+    if (*logn > MAX_LOG_LDE_TRACE)
+        return fail(TVMC_ERR_UNSUPPORTED, "LDE trace length 2^%d exceeds 2^%d", *logn, MAX_LOG_LDE_TRACE);
+    if (*le > 4) return fail(TVMC_ERR_UNSUPPORTED, "expansion factor 2^%d exceeds 16", *le);
+    return TVMC_OK;
+}
 
 int tvmc::set_error(int code, const char* msg) {
     g_err = msg;
@@ -763,6 +791,7 @@ int tvmc_set_tuning(const char* key, long long value) {
         if (value != 0 && value != 2 && value != 3) return fail(TVMC_ERR_INVALID, "lde_mid_ctas must be 0, 2 or 3");
         g_tune_mid_ctas = value;
     } else if (!strcmp(key, "hash_unfused_tree")) g_tune_unfused_tree = value ? 1 : 0;
+    else if (!strcmp(key, "fail_alloc_after")) g_fail_alloc_after = value;
     else return fail(TVMC_ERR_INVALID, "unknown tuning key '%s'", key);
     return TVMC_OK;
 }
@@ -774,7 +803,16 @@ int tvmc_get_tuning(const char* key, long long* value) {
     else if (!strcmp(key, "batch_streams")) *value = g_tune_batch_streams;
     else if (!strcmp(key, "lde_mid_ctas")) *value = g_tune_mid_ctas;
     else if (!strcmp(key, "hash_unfused_tree")) *value = g_tune_unfused_tree;
-    else return fail(TVMC_ERR_INVALID, "unknown tuning key '%s'", key);
+    else if (!strcmp(key, "fail_alloc_after")) *value = g_fail_alloc_after;
+    else if (!strcmp(key, "pool_used_bytes")) {
+        int dev;
+        cudaMemPool_t pool;
+        size_t used = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetDefaultMemPool(&pool, dev));
+        CK(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used));
+        *value = (long long)used;
+    } else return fail(TVMC_ERR_INVALID, "unknown tuning key '%s'", key);
     return TVMC_OK;
 }
 
@@ -1010,7 +1048,7 @@ int tvmc_merkle_root_gpu(const uint64_t* d_leaves, uint64_t* d_root, size_t num_
         return fail(TVMC_ERR_INVALID, "Number of leaves must be a power of 2 (got %zu)", num_leaves);
     cudaStream_t st = as_stream(stream);
     uint64_t* tree = nullptr;
-    CK(cudaMallocAsync((void**)&tree, (2 * num_leaves - 1) * 40, st));
+    CK(dev_malloc_async((void**)&tree, (2 * num_leaves - 1) * 40, st));
     cudaError_t e = launch_merkle_tree(d_leaves, tree, num_leaves, LAYOUT_FLAT, st);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(d_root, tree + 5 * (2 * num_leaves - 2), 40, cudaMemcpyDeviceToDevice, st);
@@ -1103,10 +1141,10 @@ int tvmc_commit_randomized(const uint64_t* trace, size_t trace_len, size_t width
     // host would stall while the driver maps memory).  Work on the stream runs in
     // order, so the next commit reuses it only after this one's hash.
     c->lde_borrowed = width && !frugal && (flags & TVMC_DISCARD_LDE);
-    if (cudaMallocAsync((void**)&c->d_nodes, 2 * c->L * 40, st) != cudaSuccess ||
+    if (dev_malloc_async((void**)&c->d_nodes, 2 * c->L * 40, st) != cudaSuccess ||
         (width && !frugal &&
          (c->lde_borrowed ? stream_scratch(st, c->L * width, &c->d_lde, 3) != TVMC_OK
-                          : cudaMallocAsync((void**)&c->d_lde, c->L * width * 8, st) != cudaSuccess))) {
+                          : dev_malloc_async((void**)&c->d_lde, c->L * width * 8, st) != cudaSuccess))) {
         cudaGetLastError();
         if (c->lde_borrowed) c->d_lde = nullptr;
         return bail(fail(TVMC_ERR_NOMEM, "cannot allocate LDE (%zu x %zu) and tree", c->L, width));
@@ -1120,7 +1158,7 @@ int tvmc_commit_randomized(const uint64_t* trace, size_t trace_len, size_t width
     if (R) {
         const uint64_t* src_r = randomizers;
         if (!(flags & TVMC_TRACE_DEVICE)) {
-            if (cudaMallocAsync((void**)&d_rnd, width * R * 8, st) != cudaSuccess ||
+            if (dev_malloc_async((void**)&d_rnd, width * R * 8, st) != cudaSuccess ||
                 cudaMemcpyAsync(d_rnd, randomizers, width * R * 8, cudaMemcpyHostToDevice, st) != cudaSuccess) {
                 if (d_rnd) cudaFreeAsync(d_rnd, st);
                 return bail(cuda_fail(cudaGetLastError(), "randomizer upload"));
@@ -1164,12 +1202,12 @@ int tvmc_commit_randomized(const uint64_t* trace, size_t trace_len, size_t width
         uint64_t* d_cm = nullptr;
         cudaError_t e = cudaSuccess;
         if (!dev) {
-            e = cudaMallocAsync((void**)&d_up, NW * 8, st);
+            e = dev_malloc_async((void**)&d_up, NW * 8, st);
             if (e == cudaSuccess) e = cudaMemcpyAsync(d_up, trace, NW * 8, cudaMemcpyHostToDevice, st);
             d_src = d_up;
         }
         if (e == cudaSuccess && rm) {
-            e = cudaMallocAsync((void**)&d_cm, NW * 8, st);
+            e = dev_malloc_async((void**)&d_cm, NW * 8, st);
             if (e == cudaSuccess) e = launch_transpose(d_src, width, d_cm, trace_len, trace_len, width, st);
             d_src = d_cm;
         }
@@ -1246,7 +1284,7 @@ int tvmc_commit_rows(const uint64_t* table, size_t num_rows, size_t width, uint3
         return code;
     };
     const size_t NW = num_rows * width;
-    if (cudaMallocAsync((void**)&c->d_nodes, 2 * num_rows * 40, st) != cudaSuccess ||
+    if (dev_malloc_async((void**)&c->d_nodes, 2 * num_rows * 40, st) != cudaSuccess ||
         cudaMemsetAsync(c->d_nodes, 0, 40, st) != cudaSuccess) {
         cudaGetLastError();
         return bail(fail(TVMC_ERR_NOMEM, "cannot allocate the tree of %zu leaves", num_rows));
@@ -1256,9 +1294,9 @@ int tvmc_commit_rows(const uint64_t* table, size_t num_rows, size_t width, uint3
     const uint64_t* src = table;
     if (width && !(dev && !rm && discard)) {
         uint64_t* up = nullptr;
-        cudaError_t e = cudaMallocAsync((void**)&c->d_lde, NW * 8, st);
+        cudaError_t e = dev_malloc_async((void**)&c->d_lde, NW * 8, st);
         if (e == cudaSuccess && !dev && rm) {
-            e = cudaMallocAsync((void**)&up, NW * 8, st);
+            e = dev_malloc_async((void**)&up, NW * 8, st);
             if (e == cudaSuccess) e = cudaMemcpyAsync(up, table, NW * 8, cudaMemcpyHostToDevice, st);
             if (e == cudaSuccess) e = launch_transpose(up, width, c->d_lde, num_rows, num_rows, width, st);
         } else if (e == cudaSuccess && rm) {
@@ -1300,7 +1338,7 @@ int tvmc_commit_digests(const uint64_t* leaves, size_t num_leaves, uint32_t flag
         tvmc_commitment_free(c);
         return code;
     };
-    if (cudaMallocAsync((void**)&c->d_nodes, 2 * num_leaves * 40, st) != cudaSuccess ||
+    if (dev_malloc_async((void**)&c->d_nodes, 2 * num_leaves * 40, st) != cudaSuccess ||
         cudaMemsetAsync(c->d_nodes, 0, 40, st) != cudaSuccess) {
         cudaGetLastError();
         return bail(fail(TVMC_ERR_NOMEM, "cannot allocate the tree of %zu leaves", num_leaves));
@@ -1309,7 +1347,7 @@ int tvmc_commit_digests(const uint64_t* leaves, size_t num_leaves, uint32_t flag
     uint64_t* up = nullptr;
     cudaError_t e = cudaSuccess;
     if (!(flags & TVMC_TRACE_DEVICE)) {
-        e = cudaMallocAsync((void**)&up, num_leaves * words * 8, st);
+        e = dev_malloc_async((void**)&up, num_leaves * words * 8, st);
         if (e == cudaSuccess) e = cudaMemcpyAsync(up, leaves, num_leaves * words * 8, cudaMemcpyHostToDevice, st);
         src = up;
     }
@@ -1528,9 +1566,9 @@ int tvmc_batch_create(const tvmc_table_shape* shapes, size_t count, tvmc_batch**
         c->L = s.trace_len * s.expansion;
         b->tables.push_back(c);
         uint64_t* in = nullptr;
-        if (cudaMalloc((void**)&c->d_nodes, 2 * c->L * 40) != cudaSuccess ||
-            (s.width && cudaMalloc((void**)&c->d_lde, c->L * s.width * 8) != cudaSuccess) ||
-            (s.width && cudaMalloc((void**)&in, s.trace_len * s.width * 8) != cudaSuccess)) {
+        if (dev_malloc((void**)&c->d_nodes, 2 * c->L * 40) != cudaSuccess ||
+            (s.width && dev_malloc((void**)&c->d_lde, c->L * s.width * 8) != cudaSuccess) ||
+            (s.width && dev_malloc((void**)&in, s.trace_len * s.width * 8) != cudaSuccess)) {
             cudaGetLastError();
             if (in) cudaFree(in);
             return bail(fail(TVMC_ERR_NOMEM, "cannot allocate table %zu of the batch", i));
@@ -1544,7 +1582,7 @@ int tvmc_batch_create(const tvmc_table_shape* shapes, size_t count, tvmc_batch**
         size_t words = 0;
         for (size_t i : assign[w]) words = std::max(words, lde_scratch_words(plans[i].logn, plans[i].log_exp, chunk[i]));
         uint64_t* p = nullptr;
-        if (words && cudaMalloc((void**)&p, words * 8) != cudaSuccess) {
+        if (words && dev_malloc((void**)&p, words * 8) != cudaSuccess) {
             cudaGetLastError();
             return bail(fail(TVMC_ERR_NOMEM, "cannot allocate batch scratch"));
         }
@@ -1603,6 +1641,7 @@ int tvmc_batch_input(tvmc_batch* b, size_t i, uint64_t** d_trace) {
 int tvmc_batch_run(tvmc_batch* b, void* stream) {
     if (!b) return fail(TVMC_ERR_INVALID, "null batch");
     cudaStream_t st = as_stream(stream);
+    NvtxRange range("tvmc batch launch");
     CK(cudaGraphLaunch(b->exec, st));
     g_launches.fetch_add(b->kernels_per_run);
     for (auto* c : b->tables) {

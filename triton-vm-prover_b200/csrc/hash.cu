@@ -386,6 +386,7 @@ cudaError_t launch_hash_rows(const uint64_t* table, uint64_t rstride, uint64_t c
                              uint32_t width, uint64_t* digests, uint64_t* tree, int layout,
                              cudaStream_t st) {
     if (rows == 0) return cudaSuccess;
+    NvtxRange range("tvmc row hash + Merkle tree");
     if (tree == nullptr) {
         count_launch();
         k_hash_rows<<<grid_for(rows, HASH_THREADS), HASH_THREADS, 0, st>>>(table, rstride, cstride, rows, width,
@@ -476,6 +477,7 @@ cudaError_t launch_gather_rows(const uint64_t* table, uint64_t ld, uint32_t widt
 
 cudaError_t launch_absorb_stripe(const uint64_t* stripe, uint64_t L, uint32_t ncols, uint64_t* cap, int first,
                                  int last, uint64_t* tree, cudaStream_t st) {
+    NvtxRange range("tvmc frugal stripe absorb");
     const unsigned threads = (unsigned)(L < HASH_THREADS ? L : HASH_THREADS);
     const int lt = 63 - __builtin_clzll(threads);
     const int fuse = last ? (lt < tuning_hash_fuse_levels() ? lt : tuning_hash_fuse_levels()) : 0;

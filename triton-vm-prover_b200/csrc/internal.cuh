@@ -1,15 +1,33 @@
 // Internal launcher declarations shared by the CUDA translation units.
 #pragma once
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <cstdint>
 #include <cstddef>
 
 namespace tvmc {
 
+// NVTX range around the host-side enqueue of one phase (LDE, row hash, tree,
+// frugal stripe, batch, serving commit), so that a timeline profiler groups each
+// phase's kernels under its name -- the counterpart of the reference's
+// TRITON_VM_PROFILE phase timers (include/common/debug_control.hpp).  Without
+// an attached profiler an NVTX push/pop is a no-op call.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
+
 // Number of kernels this library has launched (all devices, all threads).
 void count_launch();
 // Records `msg` as the calling thread's tvmc_last_error() text; returns code.
 int set_error(int code, const char* msg);
+// Validates the sizes of an LDE from trace_len to extended_len rows (both
+// powers of two, trace_len <= 2^MAX_LOG_LDE_TRACE, expansion <= 16) and returns
+// their logs; on failure records the message and returns the status, as every
+// LDE entry point reports it.
+int check_lde_sizes(size_t trace_len, size_t extended_len, int* logn, int* le);
 // Tuning knob "lde_mid_ctas" (2 or 3 resident CTAs per SM for the fused LDE
 // middle kernel; default 2).
 int tuning_lde_mid_ctas();

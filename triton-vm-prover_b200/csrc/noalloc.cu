@@ -12,8 +12,9 @@
 //
 // The array g_noalloc_scratch (TVMC_NOALLOC_SCRATCH_WORDS words = 64 MiB) is
 // resident on every GPU that loads the library, until the process exits.
-// Its first NOALLOC_TABLE_WORDS words hold the twiddle and coset-scale tables
-// that each call rewrites for its own size and offset; the rest holds the
+// Its first NOALLOC_TABLE_WORDS words hold the twiddle and coset-scale tables,
+// rewritten by a small kernel whenever a call's size, expansion or offset
+// differs from the previous call's on that device; the rest holds the
 // four-step intermediates.  Nothing in it needs to start at zero: every word a
 // call reads was written earlier by the same call.  All calls share the
 // array, so calls whose work overlaps on the GPU (different streams, or
@@ -47,6 +48,16 @@ static __device__ __align__(256) uint64_t g_noalloc_scratch[NOALLOC_TOTAL_WORDS]
 constexpr int MAX_DEVICES = 64;
 uint64_t* g_base[MAX_DEVICES] = {};
 std::mutex g_setup_mu;
+// The (logn, le, offset) whose tables the array holds on each device, or
+// logn = -1 before the first call.  A call with the same parameters skips the
+// table kernel: under the one-stream rule every earlier call's work, its table
+// writes included, comes before this call's kernels on the GPU, and the tables
+// region is written by the table kernel alone.
+struct TableKey {
+    int logn = -1, le = -1;
+    uint64_t offset = 0;
+};
+TableKey g_tables[MAX_DEVICES];
 
 // Formats the message into a stack buffer and hands it to tvmc_last_error().
 int fail(int code, const char* fmt, ...) {
@@ -116,17 +127,9 @@ extern "C" int tvmc_lde_batch_noalloc_gpu(const uint64_t* d_traces, size_t num_c
                                           uint64_t extended_offset, void* stream) {
     using namespace tvmc;
     (void)trace_offset;  // ignored, as in tvmc_lde_batch_gpu and the reference's LDE::extend_column
-    auto pow2 = [](size_t n) { return n != 0 && (n & (n - 1)) == 0; };
-    if (!pow2(trace_len)) return fail(TVMC_ERR_INVALID, "trace length %zu is not a power of 2", trace_len);
-    if (!pow2(extended_len) || extended_len < trace_len)
-        return fail(TVMC_ERR_INVALID, "extended length %zu is not a power of 2 >= trace length", extended_len);
-    int logn = 0, logl = 0;
-    while ((size_t(1) << logn) < trace_len) logn++;
-    while ((size_t(1) << logl) < extended_len) logl++;
-    const int le = logl - logn;
-    if (logn > MAX_LOG_LDE_TRACE)
-        return fail(TVMC_ERR_UNSUPPORTED, "trace length 2^%d exceeds 2^%d", logn, MAX_LOG_LDE_TRACE);
-    if (le > 4) return fail(TVMC_ERR_UNSUPPORTED, "expansion factor 2^%d exceeds 16", le);
+    int logn = 0, le = 0;
+    int rc = check_lde_sizes(trace_len, extended_len, &logn, &le);  // the allocating entry point's rules
+    if (rc) return rc;
     const size_t per_col = lde_scratch_words(logn, le, 1);
     if (per_col > NOALLOC_WORK_WORDS)
         return fail(TVMC_ERR_UNSUPPORTED,
@@ -139,13 +142,24 @@ extern "C" int tvmc_lde_batch_noalloc_gpu(const uint64_t* d_traces, size_t num_c
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return fail(TVMC_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
     uint64_t* base = nullptr;
-    int rc = setup_device(dev, &base);
-    if (rc) return rc;
+    if ((rc = setup_device(dev, &base))) return rc;
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
 
-    count_launch();
-    k_noalloc_tables<<<98, 1024, 0, st>>>(base, logn, le, extended_offset % GL_P);
-    if ((e = cudaGetLastError()) != cudaSuccess) return fail(TVMC_ERR_CUDA, "table kernel: %s", cudaGetErrorString(e));
+    const uint64_t off = extended_offset % GL_P;
+    {
+        std::lock_guard<std::mutex> lk(g_setup_mu);
+        TableKey& k = g_tables[dev];
+        if (k.logn != logn || k.le != le || k.offset != off) {
+            k.logn = -1;  // invalid until the table kernel is enqueued
+            count_launch();
+            k_noalloc_tables<<<98, 1024, 0, st>>>(base, logn, le, off);
+            if ((e = cudaGetLastError()) != cudaSuccess)
+                return fail(TVMC_ERR_CUDA, "table kernel: %s", cudaGetErrorString(e));
+            k.logn = logn;
+            k.le = le;
+            k.offset = off;
+        }
+    }
 
     LdePlan pl;
     pl.logn = logn;

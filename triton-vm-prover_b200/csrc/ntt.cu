@@ -732,6 +732,7 @@ cudaError_t launch_ntt(const LdePlan& pl, int inverse, uint64_t* data, uint64_t 
     const uint64_t* tw12 = pl.tw12_f;  // the inverse negates the sub-DFT input indices instead
     const uint64_t scale = (inverse && l > 0) ? GL_P - ((GL_P - 1) >> l) : 1;  // n^-1 = p - (p-1)/n
     if (cols == 0 || l == 0) return cudaSuccess;  // size-1 transform is the identity
+    NvtxRange range(inverse ? "tvmc inverse NTT" : "tvmc forward NTT");
     if (l <= 11) {
         const int lT = choose_lT(l, 11);
         const int T = 1 << lT;
@@ -788,6 +789,7 @@ cudaError_t launch_lde(const LdePlan& pl, const uint64_t* trace, uint64_t tld, u
     const int l = pl.logn, le = pl.log_exp;
     const int hi_len = l > 12 ? (1 << (l - 12)) : 1;
     if (cols == 0) return cudaSuccess;
+    NvtxRange range("tvmc LDE");
     if (l <= 11) {
         if (l == 0) {
             const uint64_t total = cols << le;

@@ -139,7 +139,6 @@ SIGNATURES = {
     "tvmc_server_destroy": (ctypes.c_int, [_vp]),
     "tvmc_set_tuning": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_longlong]),
     "tvmc_get_tuning": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_longlong)]),
-    "tvmc_int_peak_probe": (ctypes.c_double, [_vp]),
 }
 
 _lib = None
