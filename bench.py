@@ -315,6 +315,123 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_reference_gpu(args):
+    """The reference's own CUDA kernels for this path (oracle/_ref/libtvm_ref_gpu.so,
+    compiled unchanged for sm_100a) on the same workload and GPU: batched
+    randomized LDE with no randomizers (the plain LDE), hash_bfield_rows_gpu /
+    hash_xfield_rows_gpu and merkle_tree_gpu, traces resident in HBM, each
+    stage timed with CUDA events on the launching stream.  A 2^10 x 379 commit
+    through the same kernels is checked against the oracle's root first."""
+    import ctypes
+    import torch
+    from oracle import HERE as ORACLE_DIR, Oracle
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    path = os.path.join(ORACLE_DIR, "_ref", "libtvm_ref_gpu.so")
+    if not os.path.exists(path):
+        print(json.dumps({"impl": "reference", "workload": "reference GPU kernels",
+                          "unavailable": f"{path} not built (make -C oracle refgpu needs the reference tree)"}))
+        return
+    R = ctypes.CDLL(path)
+    vp, sz = ctypes.c_void_p, ctypes.c_size_t
+    R.tvmrg_lde.argtypes = [vp, sz, sz, vp, sz, ctypes.c_uint64, vp, vp]
+    R.tvmrg_hash_bfield_rows.argtypes = [vp, sz, sz, vp, vp]
+    R.tvmrg_hash_xfield_rows.argtypes = [vp, sz, sz, vp, vp]
+    R.tvmrg_merkle_tree.argtypes = [vp, vp, sz, vp]
+    stream = torch.cuda.Stream(dev)
+    sp = stream.cuda_stream
+
+    def ck(rc, what):
+        if rc != 0:
+            raise RuntimeError(f"reference {what}: CUDA error {rc}")
+
+    def commit(trace, w, n, lde, scratch, dig, tree, xfe):
+        L = EXPANSION * n
+        ck(R.tvmrg_lde(trace.data_ptr(), w, n, lde.data_ptr(), L, OFFSET, scratch.data_ptr(), sp), "LDE")
+        if xfe:
+            ck(R.tvmrg_hash_xfield_rows(lde.data_ptr(), L, w // 3, dig.data_ptr(), sp), "row hash")
+        else:
+            ck(R.tvmrg_hash_bfield_rows(lde.data_ptr(), L, w, dig.data_ptr(), sp), "row hash")
+        ck(R.tvmrg_merkle_tree(dig.data_ptr(), tree.data_ptr(), L, sp), "Merkle")
+
+    # parity: the 2^10 x 379 commit against the oracle
+    o = Oracle()
+    small = np.random.default_rng(0x7E5EED01).integers(0, P, (W_MAIN, 1 << 10), dtype=np.uint64)
+    n1, L1 = 1 << 10, EXPANSION << 10
+    t1 = torch.from_numpy(small.view(np.int64)).to(dev)
+    lde1 = torch.empty(W_MAIN * L1, dtype=torch.int64, device=dev)
+    s1 = torch.empty(W_MAIN * n1, dtype=torch.int64, device=dev)
+    d1 = torch.empty(L1 * 5, dtype=torch.int64, device=dev)
+    tr1 = torch.empty((2 * L1 - 1) * 5, dtype=torch.int64, device=dev)
+    with torch.cuda.stream(stream):
+        commit(t1, W_MAIN, n1, lde1, s1, d1, tr1, False)
+    stream.synchronize()
+    exp_lde = o.lde(small)
+    got_lde = lde1.cpu().numpy().view(np.uint64).reshape(W_MAIN, L1) % P
+    exp_root = o.merkle(o.hash_rows_cm(exp_lde))[1]
+    got_root = tr1.cpu().numpy().view(np.uint64).reshape(-1, 5)[-1] % P
+    parity = {"lde_equal": bool((got_lde == exp_lde).all()), "root_equal": bool((got_root == exp_root).all())}
+    del t1, lde1, s1, d1, tr1
+
+    n = 1 << args.log_n
+    L = EXPANSION * n
+    main = random_trace(torch, W_MAIN, n, 1000, dev)
+    aux = random_trace(torch, W_AUX, n, 2000, dev)
+    lde = torch.empty(max(W_MAIN, W_AUX) * L, dtype=torch.int64, device=dev)
+    scratch = torch.empty(max(W_MAIN, W_AUX) * n, dtype=torch.int64, device=dev)
+    dig = torch.empty(L * 5, dtype=torch.int64, device=dev)
+    tree = torch.empty((2 * L - 1) * 5, dtype=torch.int64, device=dev)
+    torch.cuda.synchronize()
+
+    def step(times=None):
+        for name, t, w, xfe in (("main", main, W_MAIN, False), ("aux", aux, W_AUX, True)):
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+            ev[0].record(stream)
+            ck(R.tvmrg_lde(t.data_ptr(), w, n, lde.data_ptr(), L, OFFSET, scratch.data_ptr(), sp), "LDE")
+            ev[1].record(stream)
+            if xfe:
+                ck(R.tvmrg_hash_xfield_rows(lde.data_ptr(), L, w // 3, dig.data_ptr(), sp), "row hash")
+            else:
+                ck(R.tvmrg_hash_bfield_rows(lde.data_ptr(), L, w, dig.data_ptr(), sp), "row hash")
+            ev[2].record(stream)
+            ck(R.tvmrg_merkle_tree(dig.data_ptr(), tree.data_ptr(), L, sp), "Merkle")
+            ev[3].record(stream)
+            if times is not None:
+                times.append((name, ev))
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        recs = []
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(0) as clk:
+            e0.record(stream)
+            for _ in range(args.steps):
+                step(recs)
+            e1.record(stream)
+            torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    stages = {}
+    for name, ev in recs:
+        d = stages.setdefault(name, {"lde": [], "row_hash": [], "merkle": []})
+        d["lde"].append(ev[0].elapsed_time(ev[1]))
+        d["row_hash"].append(ev[1].elapsed_time(ev[2]))
+        d["merkle"].append(ev[2].elapsed_time(ev[3]))
+    stages = {k: {s: statistics.median(v) for s, v in d.items()} for k, d in stages.items()}
+    cells = L * (W_MAIN + W_AUX)
+    line = {"metric": METRIC, "impl": "reference", "workload": "reference GPU kernels (sm_100a build)",
+            "value": cells / (ms / 1e3), "unit": "cells/s", "ms_per_step": ms, "steps": args.steps,
+            "warmup": args.warmup, "n_gpus": 1, "higher_is_better": True, "dtype": "u64 (Goldilocks)",
+            "data": "synthetic uniform field elements",
+            "config": {"workload": f"main 2^{args.log_n}x{W_MAIN} + aux 2^{args.log_n}x{W_AUX} limbs, x4 LDE "
+                                   "(offset 7), Tip5 row hash, Merkle (two trees)", "trace_len": n, "lde_len": L,
+                       "traces": "resident in HBM", "kernels": "randomized_lde_batch_gpu_preallocated (no "
+                       "randomizers), hash_bfield_rows_gpu / hash_xfield_rows_gpu, merkle_tree_gpu"},
+            "stage_ms_per_table": stages, "parity_2p10x379_vs_oracle": parity, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def run_ours(args):
     import torch
     import tvmc
@@ -508,6 +625,9 @@ def run_ours(args):
                          "ms_per_step": sum(hash_ms) / args.steps,
                          "ms_per_table_min_max": [min(hash_ms), max(hash_ms)]},
             "roofline_commit": roof_commit,
+            "phase_ms_per_table": {name: {"lde": statistics.median(p[1] for p in phases[i::2]),
+                                          "hash_tree": statistics.median(p[2] for p in phases[i::2])}
+                                   for i, name in enumerate(("main", "aux"))},
             "roofline_lde": {"bound": "hbm", "achieved": achieved_hbm, "peak": hbm_peak, "unit": "GB/s",
                              "frac": achieved_hbm / hbm_peak, "peak_source": hbm_src,
                              "bytes": "8*N*W read + 8*4N*W written per table",
@@ -762,7 +882,9 @@ def main():
     ap.add_argument("--workload", choices=["commit", "batch", "frugal", "serving"], default="commit")
     ap.add_argument("--streams", type=int, default=1,
                     help="commit, device-timed part: main and aux on 1 or 2 streams (e2e always uses 2)")
-    ap.add_argument("--ref-max-seconds", type=float, default=600.0,
+    ap.add_argument("--reference-gpu", action="store_true",
+                    help="with --impl reference: time the reference's own CUDA kernels (sm_100a build) instead")
+    ap.add_argument("--ref-max-seconds", type=float, default=400.0,
                     help="reference arm: time budget for its full CPU steps")
     ap.add_argument("--requests", type=int, default=48, help="serving: requests per rate")
     ap.add_argument("--serve-streams", type=int, default=4)
@@ -773,7 +895,9 @@ def main():
                     help="serving: offered load as a multiple of the plain path's capacity")
     args = ap.parse_args()
     globals()["W_MAIN"], globals()["W_AUX"] = args.width_main, args.width_aux
-    if args.impl == "reference":
+    if args.impl == "reference" and args.reference_gpu:
+        run_reference_gpu(args)
+    elif args.impl == "reference":
         run_reference(args)
     elif args.workload == "batch":
         run_batch(args)

@@ -205,6 +205,13 @@ typedef struct tvmc_commitment tvmc_commitment;
  *   "batch_streams"       worker streams a tvmc_batch spreads its tables over (default 8)
  *   "lde_mid_ctas"        resident CTAs per SM for the fused LDE middle kernel: 2 (no register
  *                         spills) or 3 (a few spills); default 2
+ *   "lde_mid_variant"     1: the fused LDE middle kernel reads its twiddles from global tables per
+ *                         coset; 2: it forms the inter-pass twiddles once per CTA in shared
+ *                         memory for all cosets; default 1
+ *   "lde_split_l1"        log2 of the LDE's four-step factor n1 (1 .. 12, with log2(N) - n1 also
+ *                         in 1 .. 12); default 0 = the balanced split
+ *   "ntt_tile_log"        log2 of the words an NTT/LDE pass CTA moves per tile (11 .. 15);
+ *                         default 0 = 13
  *   "hash_unfused_tree"   1: build every Merkle level in the tree kernel instead of the lowest
  *                         eight inside the row-hash CTAs; default 0
  *   "fail_alloc_after"    fault injection for tests: k > 0 makes the k-th device allocation the

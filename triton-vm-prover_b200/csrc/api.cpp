@@ -657,7 +657,16 @@ std::atomic<long long> g_tune_mid_ctas{0};
 std::atomic<long long> g_tune_unfused_tree{0};
 }  // namespace
 
+std::atomic<long long> g_tune_mid_variant{0};
 int tvmc::tuning_lde_mid_ctas() { return g_tune_mid_ctas.load() == 3 ? 3 : 2; }
+int tvmc::tuning_lde_mid_variant() { return g_tune_mid_variant.load() == 2 ? 2 : 1; }
+std::atomic<long long> g_tune_split_l1{0};
+std::atomic<long long> g_tune_tile_log{0};
+int tvmc::tuning_lde_split_l1() { return (int)g_tune_split_l1.load(); }
+int tvmc::tuning_ntt_tile_log() {
+    const long long v = g_tune_tile_log.load();
+    return v >= 11 && v <= 15 ? (int)v : 13;
+}
 int tvmc::tuning_hash_fuse_levels() { return g_tune_unfused_tree.load() ? 0 : 8; }
 
 struct tvmc_batch {
@@ -790,6 +799,15 @@ int tvmc_set_tuning(const char* key, long long value) {
     else if (!strcmp(key, "lde_mid_ctas")) {
         if (value != 0 && value != 2 && value != 3) return fail(TVMC_ERR_INVALID, "lde_mid_ctas must be 0, 2 or 3");
         g_tune_mid_ctas = value;
+    } else if (!strcmp(key, "lde_mid_variant")) {
+        if (value > 2) return fail(TVMC_ERR_INVALID, "lde_mid_variant must be 0, 1 or 2");
+        g_tune_mid_variant = value;
+    } else if (!strcmp(key, "lde_split_l1")) {
+        if (value > 12) return fail(TVMC_ERR_INVALID, "lde_split_l1 must be 0 .. 12");
+        g_tune_split_l1 = value;
+    } else if (!strcmp(key, "ntt_tile_log")) {
+        if (value != 0 && (value < 11 || value > 15)) return fail(TVMC_ERR_INVALID, "ntt_tile_log must be 0 or 11 .. 15");
+        g_tune_tile_log = value;
     } else if (!strcmp(key, "hash_unfused_tree")) g_tune_unfused_tree = value ? 1 : 0;
     else if (!strcmp(key, "fail_alloc_after")) g_fail_alloc_after = value;
     else return fail(TVMC_ERR_INVALID, "unknown tuning key '%s'", key);
@@ -803,6 +821,9 @@ int tvmc_get_tuning(const char* key, long long* value) {
     else if (!strcmp(key, "batch_streams")) *value = g_tune_batch_streams;
     else if (!strcmp(key, "lde_mid_ctas")) *value = g_tune_mid_ctas;
     else if (!strcmp(key, "hash_unfused_tree")) *value = g_tune_unfused_tree;
+    else if (!strcmp(key, "lde_mid_variant")) *value = g_tune_mid_variant;
+    else if (!strcmp(key, "lde_split_l1")) *value = g_tune_split_l1;
+    else if (!strcmp(key, "ntt_tile_log")) *value = g_tune_tile_log;
     else if (!strcmp(key, "fail_alloc_after")) *value = g_fail_alloc_after;
     else if (!strcmp(key, "pool_used_bytes")) {
         int dev;
@@ -1149,7 +1170,7 @@ int tvmc_commit_randomized(const uint64_t* trace, size_t trace_len, size_t width
         if (c->lde_borrowed) c->d_lde = nullptr;
         return bail(fail(TVMC_ERR_NOMEM, "cannot allocate LDE (%zu x %zu) and tree", c->L, width));
     }
-    if (cudaMemsetAsync(c->d_nodes, 0, 40, st) != cudaSuccess) return bail(cuda_fail(cudaGetLastError(), "memset"));
+    if (cudaError_t e = cudaMemsetAsync(c->d_nodes, 0, 40, st); e != cudaSuccess) return bail(cuda_fail(e, "memset"));
 
     // randomizer addends (column-major [col][k], on the trace's side of the bus)
     const size_t R = width ? num_randomizers : 0;
@@ -1158,10 +1179,11 @@ int tvmc_commit_randomized(const uint64_t* trace, size_t trace_len, size_t width
     if (R) {
         const uint64_t* src_r = randomizers;
         if (!(flags & TVMC_TRACE_DEVICE)) {
-            if (dev_malloc_async((void**)&d_rnd, width * R * 8, st) != cudaSuccess ||
-                cudaMemcpyAsync(d_rnd, randomizers, width * R * 8, cudaMemcpyHostToDevice, st) != cudaSuccess) {
+            cudaError_t e = dev_malloc_async((void**)&d_rnd, width * R * 8, st);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(d_rnd, randomizers, width * R * 8, cudaMemcpyHostToDevice, st);
+            if (e != cudaSuccess) {
                 if (d_rnd) cudaFreeAsync(d_rnd, st);
-                return bail(cuda_fail(cudaGetLastError(), "randomizer upload"));
+                return bail(cuda_fail(e, "randomizer upload"));
             }
             src_r = d_rnd;
         }
@@ -1182,7 +1204,7 @@ int tvmc_commit_randomized(const uint64_t* trace, size_t trace_len, size_t width
     const bool prof = flags & TVMC_PROFILE;
     if (prof) {
         for (auto& ev : c->prof)
-            if (cudaEventCreate(&ev) != cudaSuccess) return bail(cuda_fail(cudaGetLastError(), "event"));
+            if (cudaError_t e = cudaEventCreate(&ev); e != cudaSuccess) return bail(cuda_fail(e, "event"));
         cudaEventRecord(c->prof[0], st);
     }
     const bool dev = flags & TVMC_TRACE_DEVICE, rm = flags & TVMC_TRACE_ROW_MAJOR;
@@ -1235,11 +1257,13 @@ int tvmc_commit_randomized(const uint64_t* trace, size_t trace_len, size_t width
         if (!c->lde_borrowed) cudaFreeAsync(c->d_lde, st);  // stream-ordered after the hash kernel
         c->d_lde = nullptr;
     }
-    if (cudaEventCreateWithFlags(&c->done, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventRecord(c->done, st) != cudaSuccess)
-        return bail(cuda_fail(cudaGetLastError(), "event"));
+    {
+        cudaError_t e = cudaEventCreateWithFlags(&c->done, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventRecord(c->done, st);
+        if (e != cudaSuccess) return bail(cuda_fail(e, "event"));
+    }
     if (flags & TVMC_SYNC) {
-        if (cudaEventSynchronize(c->done) != cudaSuccess) return bail(cuda_fail(cudaGetLastError(), "sync"));
+        if (cudaError_t e = cudaEventSynchronize(c->done); e != cudaSuccess) return bail(cuda_fail(e, "sync"));
     }
     *out = c;
     return TVMC_OK;
@@ -1247,14 +1271,15 @@ int tvmc_commit_randomized(const uint64_t* trace, size_t trace_len, size_t width
 
 // Shared tail of the rows/digests commitments: completion event, optional sync.
 static int finish_commitment(tvmc_commitment* c, uint32_t flags, tvmc_commitment** out) {
-    if (cudaEventCreateWithFlags(&c->done, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventRecord(c->done, c->stream) != cudaSuccess) {
-        const int rc = cuda_fail(cudaGetLastError(), "event");
+    cudaError_t e = cudaEventCreateWithFlags(&c->done, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventRecord(c->done, c->stream);
+    if (e != cudaSuccess) {
+        const int rc = cuda_fail(e, "event");
         tvmc_commitment_free(c);
         return rc;
     }
-    if ((flags & TVMC_SYNC) && cudaEventSynchronize(c->done) != cudaSuccess) {
-        const int rc = cuda_fail(cudaGetLastError(), "sync");
+    if ((flags & TVMC_SYNC) && (e = cudaEventSynchronize(c->done)) != cudaSuccess) {
+        const int rc = cuda_fail(e, "sync");
         tvmc_commitment_free(c);
         return rc;
     }

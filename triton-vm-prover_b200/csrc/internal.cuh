@@ -31,6 +31,16 @@ int check_lde_sizes(size_t trace_len, size_t extended_len, int* logn, int* le);
 // Tuning knob "lde_mid_ctas" (2 or 3 resident CTAs per SM for the fused LDE
 // middle kernel; default 2).
 int tuning_lde_mid_ctas();
+// Tuning knob "lde_mid_variant": 1 = k_lde_mid_sym (twiddles from global tables
+// per coset), 2 = k_lde_mid_sym2 (inter-pass twiddles shared across cosets in
+// shared memory); 0 = the default.
+int tuning_lde_mid_variant();
+// Tuning knob "lde_split_l1": log2 of the four-step factor n1 of the LDE (the
+// K2 transform size), 0 = balanced; invalid values fall back to balanced.
+int tuning_lde_split_l1();
+// Tuning knob "ntt_tile_log": log2 of the words one NTT/LDE pass CTA moves per
+// tile (sequences per CTA = 2^(tile - log2 size), clamped); default 13.
+int tuning_ntt_tile_log();
 // Merkle levels built inside the row-hash CTA (8 by default; 0 with the tuning
 // knob "hash_unfused_tree" = 1); the rest are built by k_merkle_up.
 int tuning_hash_fuse_levels();

@@ -607,6 +607,100 @@ __global__ void __launch_bounds__(128, MINB) k_lde_mid_sym(const uint64_t* Y, ui
     }
 }
 
+// K2, table-sharing form of k_lde_mid_sym: the inter-pass twiddles
+// w_N^(k2*q) are the same for all E cosets, so the CTA forms them once into
+// shared memory (twq, T*n1 words) and every coset reads them there; the coset
+// scale N^-1 s_c^i, i = i0 + n2*R*k1 with i0 = k2 + n2*ln, is split into a
+// per-thread factor A_c = N^-1 s_c^i0 (one per coset) and a per-CTA table
+// sb[c][k1] = s_c^(n2*R*k1); the sub-transform twiddles come from the global
+// w_4096 table through L1.  Per element and coset this replaces four global
+// table loads and one general product by two shared-memory loads.
+template <int L1, int MINB, bool RAND>
+__global__ void __launch_bounds__(128, MINB) k_lde_mid_sym2(const uint64_t* Y, uint64_t yld, uint64_t* Z, int l2,
+                                                            int le, const uint64_t* tw12_f, const uint64_t* wlo,
+                                                            const uint64_t* whi, const uint64_t* sc_lo,
+                                                            const uint64_t* sc_hi, int hi_len, const uint64_t* add,
+                                                            int rm) {
+    using PL = Plan<L1>;
+    static_assert(PL::NR == 2 && PL::b1 == PL::b2, "square sizes only");
+    constexpr int B = PL::b1, R = 1 << B;
+    constexpr int lT = 7 - B, T = 1 << lT;  // T * R = 128 threads
+    constexpr int n1 = 1 << L1;
+    extern __shared__ uint64_t sm[];
+    uint64_t* s = sm;                          // transposes
+    uint64_t* twq = s + spad_words(n1, lT);    // w_N^((k20 + tt) * q) at [tt + T*q]
+    uint64_t* sb = twq + (T << L1);            // s_c^(n2*R*k1) at [c*R + k1]
+    const int E = 1 << le;
+    const uint64_t col = blockIdx.y;
+    const uint32_t k20 = blockIdx.x << lT;
+    const uint64_t N = 1ull << (L1 + l2);
+    for (int idx = threadIdx.x; idx < (T << L1); idx += blockDim.x)
+        twq[idx] = tw2(wlo, whi, (k20 + (idx & (T - 1))) * (uint32_t)(idx >> lT));
+    for (int idx = threadIdx.x; idx < (E << B); idx += blockDim.x) {
+        const int c = idx >> B, k1 = idx & (R - 1);
+        // tw2 on the scale tables carries N^-1; multiplying by N cancels it
+        sb[idx] = gl_mul_c(tw2(sc_lo + 4096 * c, sc_hi + hi_len * c, ((uint32_t)k1 << (B + l2))), N);
+    }
+    __syncthreads();
+    const uint64_t* src = Y + col * yld + ((uint64_t)k20 << L1);
+    const int t = threadIdx.x & (T - 1), ln = threadIdx.x >> lT;
+    const uint32_t i0 = ((uint32_t)ln << l2) + k20 + t;
+    uint64_t cf[R];  // coefficients c[R*k1 + ln] of row k20 + t
+#pragma unroll 1
+    for (int pass = 0; pass <= E; pass++) {  // 0: inverse; c + 1: forward, coset c
+        const int c = pass ? pass - 1 : 0;
+        const uint64_t a_c = tw2(sc_lo + 4096 * c, sc_hi + hi_len * c, i0);
+#pragma unroll 1
+        for (int half = 0; half < 2; half++) {
+            uint64_t v[R];
+            if (half == 0) {
+                if (pass == 0) {  // inverse round 1: elements -(ln + R*j) of row t
+#pragma unroll
+                    for (int j = 0; j < R; j++) v[j] = src[((uint64_t)t << L1) + (-(ln + (j << B)) & (n1 - 1))];
+                } else {  // forward round 1: c[ln + R*k1] * A_c * sb[c][k1]
+#pragma unroll
+                    for (int k1 = 0; k1 < R; k1++) {
+                        uint64_t x = cf[k1];
+                        if constexpr (RAND) {
+                            const uint32_t i = i0 + ((uint32_t)k1 << (B + l2));
+                            if (i < (uint32_t)rm) x = gl_add_pc(x, add[(col * E + c) * rm + i]);
+                        }
+                        v[k1] = gl_mul_c(gl_mul(x, sb[c * R + k1]), a_c);
+                    }
+                }
+            } else {  // round 2 of either: slots x + R*ln
+#pragma unroll
+                for (int x = 0; x < R; x++) v[x] = s[spos(x + (ln << B), lT) + t];
+            }
+            reg_dft<B>(v);
+            if (half == 0) {  // twiddle w_n1^(ln*k), slot ln + R*k
+#pragma unroll
+                for (int k = 0; k < R; k++) {
+                    uint64_t x = v[brevc<B>(k)];
+                    if (ln * k) x = gl_mul_c(x, __ldg(tw12_f + ((ln * k) << (12 - L1))));
+                    s[spos(ln + (k << B), lT) + t] = x;
+                }
+            } else if (pass == 0) {
+#pragma unroll
+                for (int k1 = 0; k1 < R; k1++) cf[k1] = v[brevc<B>(k1)];
+            } else {  // X[R*q1 + ln] stays in slot q1 + R*ln
+#pragma unroll
+                for (int q1 = 0; q1 < R; q1++) s[spos(q1 + (ln << B), lT) + t] = v[brevc<B>(q1)];
+            }
+            __syncthreads();
+        }
+        if (pass) {
+            uint64_t* dst = Z + (col * E + c) * N + k20;
+            for (int idx = threadIdx.x; idx < (T << L1); idx += blockDim.x) {
+                const int tt = idx & (T - 1), q = idx >> lT;
+                const uint64_t x = s[spos((q >> B) + ((q & (R - 1)) << B), lT) + tt];
+                dst[tt + ((uint64_t)q << l2)] = gl_mul_c(x, twq[idx]);
+            }
+            __syncthreads();
+        }
+    }
+}
+
 // K3: for q2 in [q20, q20+T3), all E cosets: DFT_n2 over rows Z_c[i1' + n2*q2];
 // E_c[n1*q1 + q2] -> LDE[E*(n1*q1 + q2) + c], written as runs of E*T3 words.
 // Sequence u = E*t + c of the CTA is row q20 + t of coset c.
@@ -696,6 +790,14 @@ static int choose_lT(int ls, int budget_words_log) {
     return clampi(budget_words_log - ls, 0, ls <= 5 ? 8 : 3);
 }
 
+// The largest lT' <= lT whose tile fits in one CTA's shared memory: the
+// 2^ls-word twiddle table plus nbuf transpose buffers of 2^(lT' + extra)
+// sequences (extra: the E cosets K3 moves per sequence).
+static int fit_lT(int lT, int ls, int nbuf, int extra = 0) {
+    while (lT > 0 && ((size_t)(1u << ls) + (size_t)nbuf * spad_words(1 << ls, lT + extra)) * 8 > 227 * 1024) lT--;
+    return lT;
+}
+
 static cudaError_t set_smem(const void* fn, size_t bytes) {
     if (bytes > 48 * 1024)
         return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
@@ -750,7 +852,8 @@ cudaError_t launch_ntt(const LdePlan& pl, int inverse, uint64_t* data, uint64_t 
     const uint64_t n = 1ull << l;
     const uint64_t* wlo = inverse ? pl.wn_i_lo : pl.wn_f_lo;
     const uint64_t* whi = inverse ? pl.wn_i_hi : pl.wn_f_hi;
-    const int lTa = choose_lT(l2, 13), lTb = choose_lT(l1, 13);
+    const int tile = tuning_ntt_tile_log();
+    const int lTa = fit_lT(choose_lT(l2, tile), l2, 1), lTb = fit_lT(choose_lT(l1, tile), l1, 1);
     const size_t smem_a = words_bytes((1u << l2) + spad_words(1 << l2, lTa));
     const size_t smem_b = words_bytes((1u << l1) + spad_words(1 << l1, lTb));
     for (uint64_t c0 = 0; c0 < cols; c0 += 65535) {
@@ -809,13 +912,19 @@ cudaError_t launch_lde(const LdePlan& pl, const uint64_t* trace, uint64_t tld, u
             return cudaGetLastError();
         });
     }
-    const int l1 = (l + 1) / 2, l2 = l / 2;
+    // four-step split N = n1 * n2 (K2 runs the n1-point transforms, K1 and K3
+    // the n2-point ones); the default is the balanced split, the tuning knob
+    // "lde_split_l1" picks another valid one
+    int l1 = (l + 1) / 2;
+    if (const int ks = tuning_lde_split_l1(); ks >= 1 && ks <= 12 && l - ks >= 1 && l - ks <= 12) l1 = ks;
+    const int l2 = l - l1;
+    const int tile = tuning_ntt_tile_log();
     const uint64_t N = 1ull << l;
-    const int lT1 = choose_lT(l2, 13);
+    const int lT1 = fit_lT(choose_lT(l2, tile), l2, 1);
     const size_t smem1 = words_bytes((1u << l2) + spad_words(1 << l2, lT1));
-    const int lT2 = choose_lT(l1, 13);
+    const int lT2 = fit_lT(choose_lT(l1, tile), l1, 2);
     const size_t smem2 = words_bytes((size_t)(1u << l1) + 2 * spad_words(1 << l1, lT2));
-    const int lT3 = clampi(13 - l2 - le, 0, 1);
+    const int lT3 = fit_lT(clampi(tile - l2 - le, 0, 1), l2, 1, le);
     const size_t smem3 = words_bytes((1u << l2) + spad_words(1 << l2, lT3 + le));
     uint64_t* Y = scratch;
     for (uint64_t c0 = 0; c0 < cols; c0 += 65535) {
@@ -834,6 +943,19 @@ cudaError_t launch_lde(const LdePlan& pl, const uint64_t* trace, uint64_t tld, u
         e = dispatch_ls(l1, [&]<int L1>() -> cudaError_t {
             if constexpr (Plan<L1>::NR == 2 && Plan<L1>::b1 == Plan<L1>::b2) {
                 constexpr int lTr = 7 - Plan<L1>::b2;
+                if (tuning_lde_mid_variant() == 2) {
+                    const size_t sm2 = words_bytes(spad_words(1 << L1, lTr) + ((size_t)1 << (lTr + L1)) +
+                                                   ((size_t)1 << (le + Plan<L1>::b2)));
+                    auto kern = rm ? k_lde_mid_sym2<L1, 2, true>
+                                   : (tuning_lde_mid_ctas() == 3 ? k_lde_mid_sym2<L1, 3, false>
+                                                                 : k_lde_mid_sym2<L1, 2, false>);
+                    cudaError_t e2 = set_smem((const void*)kern, sm2);
+                    if (e2 != cudaSuccess) return e2;
+                    count_launch();
+                    kern<<<dim3((1u << l2) >> lTr, nc), 128, sm2, st>>>(
+                        Y, N, Z, l2, le, pl.tw12_f, pl.wn_f_lo, pl.wn_f_hi, pl.sc_lo, pl.sc_hi, hi_len, addc, rm);
+                    return cudaGetLastError();
+                }
                 const size_t smr = words_bytes((size_t)(1u << L1) + spad_words(1 << L1, lTr));
                 // register budget: 2 resident CTAs (no spills) or 3 (a few spills); tuning knob
                 // (the randomized variant runs at 2 CTAs per SM)
