@@ -203,13 +203,15 @@ typedef struct tvmc_commitment tvmc_commitment;
  *   "lde_scratch_bytes"   LDE intermediate budget per call (default 2 GiB); columns are
  *                         processed in chunks that fit
  *   "batch_streams"       worker streams a tvmc_batch spreads its tables over (default 8)
+ *   "batch_multi_hash"    1: a tvmc_batch hashes all its tables with one multi-table launch after
+ *                         their LDEs; 2: each worker stream hashes its own tables; default 1
  *   "lde_mid_ctas"        resident CTAs per SM for the fused LDE middle kernel: 2 (no register
  *                         spills) or 3 (a few spills); default 2
  *   "lde_mid_variant"     1: the fused LDE middle kernel reads its twiddles from global tables per
  *                         coset; 2: it forms the inter-pass twiddles once per CTA in shared
  *                         memory for all cosets; default 1
- *   "lde_split_l1"        log2 of the LDE's four-step factor n1 (1 .. 12, with log2(N) - n1 also
- *                         in 1 .. 12); default 0 = the balanced split
+ *   "lde_split_l1"        log2 of the LDE's four-step factor n1 (6 .. 12, with log2(N) - n1 also
+ *                         in 6 .. 12, else the balanced split is used); default 0 = balanced
  *   "ntt_tile_log"        log2 of the words an NTT/LDE pass CTA moves per tile (11 .. 15);
  *                         default 0 = 13
  *   "hash_unfused_tree"   1: build every Merkle level in the tree kernel instead of the lowest
@@ -240,6 +242,24 @@ int tvmc_get_tuning(const char* key, long long* value);
  * tvmc_commitment_free.  Work is enqueued on `stream`. */
 int tvmc_commit(const uint64_t* trace, size_t trace_len, size_t width, uint32_t expansion, uint64_t offset,
                 uint32_t flags, void* stream, tvmc_commitment** out);
+/* Several plain commitments at once: per table the same as tvmc_commit (LDE
+ * onto offset * <w_{trace_len*expansion}>, Tip5 row hash, heap Merkle tree),
+ * but the row hashing and the small tree tops of all tables run as one launch
+ * each, so that many small tables fill the GPU together instead of one after
+ * another.  out[i] receives table i's commitment (free each with
+ * tvmc_commitment_free).  Flags: TVMC_TRACE_DEVICE (every trace is a device
+ * pointer), TVMC_DISCARD_LDE, TVMC_SYNC.  On failure no commitment is
+ * returned.  No reference counterpart (the reference commits one table at a
+ * time, src/stark.cpp:1163-1196). */
+typedef struct {
+    const uint64_t* trace; /* column-major, width x trace_len */
+    size_t trace_len;
+    size_t width;
+    uint32_t expansion;
+    uint64_t offset;
+} tvmc_multi_table;
+int tvmc_commit_multi(const tvmc_multi_table* tables, size_t count, uint32_t flags, void* stream,
+                      tvmc_commitment** out);
 /* The same commitment over the randomized (zero-knowledge) LDE of
  * LDETable::extend_table_with_randomizers / RandomizedLDE::extend_column_with_randomizer
  * (src/lde/lde_table.cpp:8-57, src/lde/lde_randomized.cpp:71-154): per column
@@ -348,7 +368,10 @@ int tvmc_batch_free(tvmc_batch* b);
  * running requests and the trees still held, and is issued at once on the
  * least-loaded of its worker streams.  Small tables (LDE up to 128 MB) run
  * concurrently on num_streams high-priority streams and never wait behind
- * large ones; large tables, each enough to fill the GPU, go in arrival order
+ * large ones; plain small requests queued at the same time are committed
+ * together as one tvmc_commit_multi (their row hashes share one launch, so a
+ * burst of small tables fills the GPU instead of trickling through it) unless
+ * TVMC_SERVER_NO_GROUPING is set; large tables, each enough to fill the GPU, go in arrival order
  * onto one dedicated stream, with up to max_large_inflight of them issued at
  * once (the next one's upload overlaps the current one's kernels).  Each request's
  * Merkle tree stays on the device for openings until tvmc_server_release;
@@ -359,11 +382,12 @@ int tvmc_batch_free(tvmc_batch* b);
 typedef struct tvmc_server tvmc_server;
 
 #define TVMC_SERVER_KEEP_LDE 0x1u
+#define TVMC_SERVER_NO_GROUPING 0x2u /* commit every small request on its own */
 
 typedef struct tvmc_server_config {
     size_t hbm_budget_bytes; /* 0: 90% of the device memory free at creation */
     uint32_t num_streams;    /* worker streams for small tables, 0: 4 (at most 64) */
-    uint32_t flags;          /* TVMC_SERVER_KEEP_LDE */
+    uint32_t flags;          /* TVMC_SERVER_KEEP_LDE, TVMC_SERVER_NO_GROUPING */
     uint32_t max_large_inflight; /* large tables issued at once, 0: 2 (at most 16) */
 } tvmc_server_config;
 

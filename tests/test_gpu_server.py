@@ -44,6 +44,51 @@ def test_server_results_equal_alone(tv, streams, budget):
             assert st["bytes_peak"] <= budget
 
 
+@pytest.mark.parametrize("group_small", [True, False])
+def test_server_mix_up_to_2p20_rows_equals_alone(tv, group_small):
+    """The serving stream's whole size range in one mix: tables of 2^18 .. 2^20
+    rows (large, on the dedicated stream) among bursts of small ones (committed
+    together as multi-table groups, or one by one): each root and a set of
+    openings equal the table committed alone."""
+    tables = _mix(31, 18, logs=(10, 11, 12, 13, 14), widths=(379, 264, 23))
+    tables.insert(3, rand_u64(3101, (379, 1 << 20)))
+    tables.insert(9, rand_u64(3102, (264, 1 << 19)))
+    tables.insert(15, rand_u64(3103, (23, 1 << 18)))
+    rng = np.random.default_rng(4)
+    with tv.Server(streams=4, group_small=group_small) as srv:
+        ids = [srv.submit(t) for t in tables]
+        for rid, t in zip(ids, tables):
+            root = srv.wait(rid)
+            idx = rng.integers(0, 4 * t.shape[1], 8)
+            with tv.Commitment(t, discard_lde=True) as alone:
+                assert (root == alone.root()).all()
+                assert (srv.open(rid, idx) == alone.auth_paths(idx)).all()
+            srv.release(rid)
+        st = srv.stats()
+        assert st["completed"] == len(tables) and st["failed"] == 0 and st["bytes_in_use"] == 0
+
+
+def test_server_groups_a_burst_of_small_requests(tv, oracle):
+    """64 small requests submitted at once while a large one runs: they are
+    committed in multi-table groups and every tree equals the oracle's."""
+    small = [rand_u64(3200 + i, (int(w), 1 << int(l)))
+             for i, (l, w) in enumerate(zip(np.random.default_rng(5).integers(0, 9, 64),
+                                            np.random.default_rng(6).choice([1, 9, 23, 379], 64)))]
+    big = rand_u64(3199, (379, 1 << 18))
+    with tv.Server(streams=2) as srv:
+        rb = srv.submit(big)
+        ids = [srv.submit(t) for t in small]
+        for rid, t in zip(ids, small):
+            exp = oracle.merkle(oracle.hash_rows_cm(oracle.lde(t)))
+            assert (srv.wait(rid) == exp[1]).all()
+            assert (srv.open(rid, [0, 4 * t.shape[1] - 1]) ==
+                    np.stack([oracle.auth_path(exp, 0), oracle.auth_path(exp, 4 * t.shape[1] - 1)])).all()
+            srv.release(rid)
+        with tv.Commitment(big, discard_lde=True) as alone:
+            assert (srv.wait(rb) == alone.root()).all()
+        srv.release(rb)
+
+
 def test_server_keep_lde_rows_and_layouts(tv):
     t = rand_u64(11, (37, 1 << 9))
     with tv.Server(keep_lde=True) as srv:

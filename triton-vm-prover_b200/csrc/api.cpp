@@ -653,6 +653,7 @@ void destroy_commitment(tvmc_commitment* c) {
     delete c;
 }
 std::atomic<long long> g_tune_batch_streams{0};
+std::atomic<long long> g_tune_batch_multi{0};  // 0 / 1: multi-table hash; 2: per-table hash
 std::atomic<long long> g_tune_mid_ctas{0};
 std::atomic<long long> g_tune_unfused_tree{0};
 }  // namespace
@@ -802,6 +803,9 @@ int tvmc_set_tuning(const char* key, long long value) {
     } else if (!strcmp(key, "lde_mid_variant")) {
         if (value > 2) return fail(TVMC_ERR_INVALID, "lde_mid_variant must be 0, 1 or 2");
         g_tune_mid_variant = value;
+    } else if (!strcmp(key, "batch_multi_hash")) {
+        if (value > 2) return fail(TVMC_ERR_INVALID, "batch_multi_hash must be 0, 1 or 2");
+        g_tune_batch_multi = value;
     } else if (!strcmp(key, "lde_split_l1")) {
         if (value > 12) return fail(TVMC_ERR_INVALID, "lde_split_l1 must be 0 .. 12");
         g_tune_split_l1 = value;
@@ -823,6 +827,7 @@ int tvmc_get_tuning(const char* key, long long* value) {
     else if (!strcmp(key, "hash_unfused_tree")) *value = g_tune_unfused_tree;
     else if (!strcmp(key, "lde_mid_variant")) *value = g_tune_mid_variant;
     else if (!strcmp(key, "lde_split_l1")) *value = g_tune_split_l1;
+    else if (!strcmp(key, "batch_multi_hash")) *value = g_tune_batch_multi;
     else if (!strcmp(key, "ntt_tile_log")) *value = g_tune_tile_log;
     else if (!strcmp(key, "fail_alloc_after")) *value = g_fail_alloc_after;
     else if (!strcmp(key, "pool_used_bytes")) {
@@ -1269,6 +1274,92 @@ int tvmc_commit_randomized(const uint64_t* trace, size_t trace_len, size_t width
     return TVMC_OK;
 }
 
+int tvmc_commit_multi(const tvmc_multi_table* tables, size_t count, uint32_t flags, void* stream,
+                      tvmc_commitment** out) {
+    if (!out || (count && !tables)) return fail(TVMC_ERR_INVALID, "null argument");
+    for (size_t i = 0; i < count; i++) out[i] = nullptr;
+    if (flags & ~(TVMC_TRACE_DEVICE | TVMC_DISCARD_LDE | TVMC_SYNC))
+        return fail(TVMC_ERR_INVALID, "tvmc_commit_multi takes TVMC_TRACE_DEVICE, TVMC_DISCARD_LDE and TVMC_SYNC");
+    if (count == 0) return TVMC_OK;
+    const bool dev = flags & TVMC_TRACE_DEVICE, discard = flags & TVMC_DISCARD_LDE;
+    cudaStream_t st = as_stream(stream);
+    std::vector<LdePlan> plans(count);
+    size_t stage_words = 0, lde_words = 0;
+    for (size_t i = 0; i < count; i++) {
+        const tvmc_multi_table& t = tables[i];
+        if (!is_pow2(t.expansion) || t.expansion > 16)
+            return fail(TVMC_ERR_INVALID, "table %zu: expansion factor %u is not a power of 2 <= 16", i, t.expansion);
+        int logn, le;
+        int rc = check_lde_sizes(t.trace_len, t.trace_len * t.expansion, &logn, &le);
+        if (rc) return rc;
+        if (t.width && !t.trace) return fail(TVMC_ERR_INVALID, "table %zu: null trace", i);
+        if ((rc = get_plan(logn, le, t.offset, &plans[i]))) return rc;
+        stage_words += dev ? 0 : t.trace_len * t.width;
+        lde_words += t.trace_len * t.expansion * t.width;
+    }
+    NvtxRange range("tvmc multi-table commit");
+    std::vector<tvmc_commitment*> cs(count, nullptr);
+    auto bail = [&](int code) {
+        for (auto* c : cs)
+            if (c) destroy_commitment(c);
+        return code;
+    };
+    uint64_t *stage = nullptr, *lde_all = nullptr;
+    int rc = stream_scratch(st, stage_words, &stage, 4);
+    if (!rc && discard) rc = stream_scratch(st, lde_words, &lde_all, 3);
+    if (rc) return rc;
+    std::vector<MultiHashTable> hjobs;
+    size_t so = 0, lo = 0;
+    for (size_t i = 0; i < count; i++) {
+        const tvmc_multi_table& t = tables[i];
+        tvmc_commitment* c = cs[i] = new tvmc_commitment();
+        c->device = -1;
+        CK(cudaGetDevice(&c->device));
+        c->stream = st;
+        c->n = t.trace_len;
+        c->width = t.width;
+        c->L = t.trace_len * t.expansion;
+        c->pooled = true;
+        if (dev_malloc_async(&c->d_nodes, 2 * c->L * 40, st) != cudaSuccess)
+            return bail(fail(TVMC_ERR_NOMEM, "table %zu: cannot allocate the tree of %zu leaves", i, c->L));
+        if (cudaError_t e = cudaMemsetAsync(c->d_nodes, 0, 40, st); e != cudaSuccess) return bail(cuda_fail(e, "memset"));
+        uint64_t* lde = nullptr;
+        if (t.width) {
+            if (discard) {
+                lde = lde_all + lo;
+                lo += c->L * t.width;
+            } else {
+                if (dev_malloc_async(&c->d_lde, c->L * t.width * 8, st) != cudaSuccess)
+                    return bail(fail(TVMC_ERR_NOMEM, "table %zu: cannot allocate its LDE", i));
+                lde = c->d_lde;
+            }
+            const uint64_t* src = t.trace;
+            if (!dev) {
+                uint64_t* d = stage + so;
+                so += t.trace_len * t.width;
+                if (cudaError_t e = cudaMemcpyAsync(d, t.trace, t.trace_len * t.width * 8, cudaMemcpyHostToDevice, st);
+                    e != cudaSuccess)
+                    return bail(cuda_fail(e, "trace upload"));
+                src = d;
+            }
+            if ((rc = run_lde(plans[i], src, t.trace_len, lde, c->L, t.width, st))) return bail(rc);
+        }
+        hjobs.push_back(MultiHashTable{lde, c->d_nodes, c->L, (uint32_t)t.width});
+    }
+    if (cudaError_t e = launch_hash_rows_multi(hjobs.data(), (int)hjobs.size(), st); e != cudaSuccess)
+        return bail(cuda_fail(e, "multi-table hash/merkle"));
+    for (size_t i = 0; i < count; i++) {
+        cudaError_t e = cudaEventCreateWithFlags(&cs[i]->done, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventRecord(cs[i]->done, st);
+        if (e != cudaSuccess) return bail(cuda_fail(e, "event"));
+    }
+    if (flags & TVMC_SYNC) {
+        if (cudaError_t e = cudaEventSynchronize(cs[count - 1]->done); e != cudaSuccess) return bail(cuda_fail(e, "sync"));
+    }
+    for (size_t i = 0; i < count; i++) out[i] = cs[i];
+    return TVMC_OK;
+}
+
 // Shared tail of the rows/digests commitments: completion event, optional sync.
 static int finish_commitment(tvmc_commitment* c, uint32_t flags, tvmc_commitment** out) {
     cudaError_t e = cudaEventCreateWithFlags(&c->done, cudaEventDisableTiming);
@@ -1622,7 +1713,10 @@ int tvmc_batch_create(const tvmc_table_shape* shapes, size_t count, tvmc_batch**
         b->events.push_back(ev);
     }
     CK(cudaStreamCreateWithFlags(&b->capture, cudaStreamNonBlocking));
-    // capture: fork -> per-worker table commits -> join
+    // capture: fork -> per-worker table commits -> join; with knob
+    // "batch_multi_hash" (default on) the workers run the LDEs only and one
+    // multi-table launch hashes every table after the join
+    const bool multi = g_tune_batch_multi.load() != 2;
     const unsigned long long k0 = g_launches.load();
     CK(cudaStreamBeginCapture(b->capture, cudaStreamCaptureModeRelaxed));
     cudaError_t e = cudaEventRecord(b->events[0], b->capture);
@@ -1638,11 +1732,21 @@ int tvmc_batch_create(const tvmc_table_shape* shapes, size_t count, tvmc_batch**
                 const size_t nc = std::min(chunk[i], W - c0);
                 e = launch_lde(plans[i], b->inputs[i] + c0 * N, N, c->d_lde + c0 * c->L, c->L, nc, b->scratch[w], st);
             }
-            if (e == cudaSuccess)
+            if (e == cudaSuccess && !multi)
                 e = launch_hash_rows(c->d_lde, 1, c->L, c->L, (uint32_t)W, nullptr, c->d_nodes, LAYOUT_HEAP, st);
         }
         if (e == cudaSuccess) e = cudaEventRecord(b->events[w + 1], st);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(b->capture, b->events[w + 1], 0);
+    }
+    if (multi && e == cudaSuccess) {
+        // after every LDE: all tables' row hashes as one launch (largest first,
+        // so that the small tables' CTAs fill the tail), then the tree tops
+        std::vector<MultiHashTable> jobs;
+        for (size_t i : order) {
+            tvmc_commitment* c = b->tables[i];
+            jobs.push_back(MultiHashTable{c->d_lde, c->d_nodes, c->L, (uint32_t)shapes[i].width});
+        }
+        e = launch_hash_rows_multi(jobs.data(), (int)jobs.size(), b->capture);
     }
     cudaGraph_t g = nullptr;
     const cudaError_t e2 = cudaStreamEndCapture(b->capture, &g);

@@ -30,11 +30,13 @@ __device__ __forceinline__ void store_digest(uint64_t* p, const uint64_t d[5]) {
     for (int i = 0; i < 5; i++) p[i] = d[i];
 }
 
-// Builds `levels` tree levels above the `count` digests held in sd (count =
-// blockDim.x), where those digests are heap nodes [base, base + count).
+// Builds `levels` tree levels above the `count` digests held in sd (count <=
+// blockDim.x, a power of two), where those digests are heap nodes
+// [base, base + count).  Every thread of the CTA must call it.
 __device__ __forceinline__ void subtree_levels(uint64_t* sd, uint64_t base, int levels, uint64_t* tree,
-                                               uint64_t n, int layout, const uint32_t* lt) {
-    int count = blockDim.x;
+                                               uint64_t n, int layout, const uint32_t* lt,
+                                               int count = -1) {
+    if (count < 0) count = blockDim.x;
     for (int lv = 1; lv <= levels; lv++) {
         count >>= 1;
         base >>= 1;
@@ -149,6 +151,87 @@ __global__ void __launch_bounds__(HASH_THREADS, HASH_CTAS_PER_SM) k_absorb_strip
         store_digest(sd + 5 * threadIdx.x, d);
         __syncthreads();
         subtree_levels(sd, L + (uint64_t)blockIdx.x * blockDim.x, fuse, tree, L, LAYOUT_HEAP, lt);
+    }
+}
+
+// ---- multi-table commitments ------------------------------------------------
+// Small tables (a few thousand rows) leave most of the GPU idle when hashed one
+// launch at a time: a 2^12-row LDE is 32 CTAs, and each row is a chain of 38
+// permutations.  These kernels take up to HASH_MULTI_MAX tables of any heights
+// and widths in one launch, so that many small commitments (the serving loop's
+// queued requests, a batch of uneven tables) fill the GPU together.
+
+// Row hash of several tables: CTA b belongs to the job j with
+// block0[j] <= b < block0[j + 1]; its rows are hashed as in k_hash_rows and
+// the lowest levels of that table's heap tree are built in shared memory.
+__global__ void __launch_bounds__(HASH_THREADS, HASH_CTAS_PER_SM) k_hash_rows_multi(const __grid_constant__ HashJobs jobs,
+                                                                                  int fuse_max) {
+    __shared__ uint32_t sbox[T5_SBOX_WORDS];
+    extern __shared__ uint64_t sd[];  // 5 * blockDim words
+    t5_sbox_init(sbox);
+    int j = 0;
+    for (int k = 1; k < jobs.count; k++)
+        if (jobs.j[k].block0 <= blockIdx.x) j = k;
+    const uint64_t* tab = jobs.j[j].lde;
+    uint64_t* tree = jobs.j[j].tree;
+    const uint64_t L = jobs.j[j].L;
+    const uint32_t width = jobs.j[j].width;
+    __syncthreads();
+    const uint32_t* lt = sbox + (threadIdx.x & 31);
+    const int active = L < blockDim.x ? (int)L : (int)blockDim.x;  // L is a power of two
+    const uint64_t row0 = (uint64_t)(blockIdx.x - jobs.j[j].block0) * blockDim.x;
+    const uint64_t row = row0 + threadIdx.x;
+    const bool live = threadIdx.x < active;
+    const uint64_t* p = tab + (live ? row : 0);
+
+    uint64_t s[T5_STATE];
+#pragma unroll
+    for (int i = 0; i < T5_STATE; i++) s[i] = 0;
+    const uint32_t full = width / T5_RATE;
+    const uint32_t rem = width - full * T5_RATE;
+    for (uint32_t k = 0; k < full; k++) {
+#pragma unroll
+        for (int i = 0; i < T5_RATE; i++) s[i] = live ? __ldg(p + (uint64_t)(k * T5_RATE + i) * L) : 0;
+        t5_permutation(s, lt);
+    }
+#pragma unroll
+    for (int i = 0; i < T5_RATE; i++)
+        s[i] = ((uint32_t)i < rem) ? (live ? __ldg(p + (uint64_t)(full * T5_RATE + i) * L) : 0)
+                                   : ((uint32_t)i == rem ? 1 : 0);
+    t5_permutation(s, lt);
+    uint64_t d[5];
+#pragma unroll
+    for (int i = 0; i < 5; i++) d[i] = gl_canon(s[i]);
+    if (live) {
+        store_digest(tree + 5 * (L + row), d);
+        store_digest(sd + 5 * threadIdx.x, d);
+    }
+    __syncthreads();
+    const int levels = min(fuse_max, 31 - __clz(active));
+    subtree_levels(sd, L + row0, levels, tree, L, LAYOUT_HEAP, lt, active);
+}
+
+// The tops of several heap trees, one CTA per tree: tree j has its level of
+// m[j] nodes (heap [m, 2m)) in place and gets every level above it.  Each
+// level is read from global memory after the barrier that follows its writes.
+__global__ void __launch_bounds__(256) k_merkle_tops_multi(const __grid_constant__ TopJobs jobs) {
+    __shared__ uint32_t sbox[T5_SBOX_WORDS];
+    t5_sbox_init(sbox);
+    __syncthreads();
+    const uint32_t* lt = sbox + (threadIdx.x & 31);
+    uint64_t* tree = jobs.j[blockIdx.x].tree;
+    for (uint64_t m = jobs.j[blockIdx.x].m; m > 1; m >>= 1) {
+        for (uint64_t par = (m >> 1) + threadIdx.x; par < m; par += blockDim.x) {
+            uint64_t a[5], b[5], h[5];
+#pragma unroll
+            for (int i = 0; i < 5; i++) {
+                a[i] = tree[5 * (2 * par) + i];
+                b[i] = tree[5 * (2 * par + 1) + i];
+            }
+            t5_hash_pair(a, b, h, lt);
+            store_digest(tree + 5 * par, h);
+        }
+        __syncthreads();
     }
 }
 
@@ -402,6 +485,47 @@ cudaError_t launch_hash_rows(const uint64_t* table, uint64_t rstride, uint64_t c
     if (e != cudaSuccess) return e;
     // the block subtrees are complete up to `fuse` levels; continue from there
     return launch_tree_above(tree, rows, rows >> fuse, layout, st);
+}
+
+cudaError_t launch_hash_rows_multi(const MultiHashTable* tabs, int count, cudaStream_t st) {
+    NvtxRange range("tvmc multi-table row hash + Merkle trees");
+    const int fuse = ilog2u(HASH_THREADS);  // every level a CTA's rows span
+    for (int c0 = 0; c0 < count; c0 += HASH_MULTI_MAX) {
+        const int nj = count - c0 < HASH_MULTI_MAX ? count - c0 : HASH_MULTI_MAX;
+        HashJobs hj{};
+        TopJobs tj{};
+        uint64_t blocks = 0;
+        int ntops = 0;
+        for (int k = 0; k < nj; k++) {
+            const MultiHashTable& t = tabs[c0 + k];
+            hj.j[k] = HashJob{t.lde, t.tree, t.L, t.width, (uint32_t)blocks};
+            blocks += (t.L + HASH_THREADS - 1) / HASH_THREADS;
+        }
+        hj.count = nj;
+        if (blocks == 0) continue;
+        count_launch();
+        k_hash_rows_multi<<<(unsigned)blocks, HASH_THREADS, 40 * HASH_THREADS, st>>>(hj, fuse);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        // above the fused levels: small remainders in one multi-tree launch, large
+        // ones with the single-tree kernels
+        for (int k = 0; k < nj; k++) {
+            const MultiHashTable& t = tabs[c0 + k];
+            const uint64_t m = t.L > HASH_THREADS ? t.L / HASH_THREADS : 1;
+            if (m <= 1) continue;
+            if (m <= MULTI_TOP_MAX_NODES) {
+                tj.j[ntops++] = TopJob{t.tree, m};
+            } else if ((e = launch_tree_above(t.tree, t.L, m, LAYOUT_HEAP, st)) != cudaSuccess) {
+                return e;
+            }
+        }
+        if (ntops) {
+            count_launch();
+            k_merkle_tops_multi<<<(unsigned)ntops, 256, 0, st>>>(tj);
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        }
+    }
+    return cudaSuccess;
 }
 
 cudaError_t launch_merkle_tree(const uint64_t* leaves, uint64_t* tree, uint64_t n, int layout,

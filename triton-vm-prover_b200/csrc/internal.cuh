@@ -36,7 +36,8 @@ int tuning_lde_mid_ctas();
 // shared memory); 0 = the default.
 int tuning_lde_mid_variant();
 // Tuning knob "lde_split_l1": log2 of the four-step factor n1 of the LDE (the
-// K2 transform size), 0 = balanced; invalid values fall back to balanced.
+// K2 transform size), 0 = balanced; a split with either factor outside
+// [2^6, 2^12] falls back to balanced.
 int tuning_lde_split_l1();
 // Tuning knob "ntt_tile_log": log2 of the words one NTT/LDE pass CTA moves per
 // tile (sequences per CTA = 2^(tile - log2 size), clamped); default 13.
@@ -84,6 +85,36 @@ cudaError_t launch_absorb_stripe(const uint64_t* stripe, uint64_t L, uint32_t nc
                                  int last, uint64_t* tree, cudaStream_t st);
 cudaError_t launch_hash_pairs(const uint64_t* left, const uint64_t* right, uint64_t* out, uint64_t count,
                               cudaStream_t st);
+
+// Multi-table row hash + heap Merkle trees (one launch for up to
+// HASH_MULTI_MAX tables, one more for the small tree tops).
+struct MultiHashTable {
+    const uint64_t* lde;  // column-major, column stride L
+    uint64_t* tree;       // heap layout, 2L digests (node 0 unused)
+    uint64_t L;           // rows, a power of two
+    uint32_t width;
+};
+constexpr int HASH_MULTI_MAX = 64;
+constexpr uint64_t MULTI_TOP_MAX_NODES = 1024;  // larger tree tops use the single-tree kernels
+struct HashJob {
+    const uint64_t* lde;
+    uint64_t* tree;
+    uint64_t L;
+    uint32_t width;
+    uint32_t block0;  // first CTA of this table
+};
+struct HashJobs {
+    HashJob j[HASH_MULTI_MAX];
+    int count;
+};
+struct TopJob {
+    uint64_t* tree;
+    uint64_t m;  // nodes of the level already in place
+};
+struct TopJobs {
+    TopJob j[HASH_MULTI_MAX];
+};
+cudaError_t launch_hash_rows_multi(const MultiHashTable* tabs, int count, cudaStream_t st);
 cudaError_t launch_tip5_permutations(uint64_t* states, uint64_t count, cudaStream_t st);
 // Fiat-Shamir absorb of [lead (if has_lead)] ++ data[0..len) into the 16-word sponge state.
 cudaError_t launch_sponge_absorb(uint64_t* state, const uint64_t* data, uint64_t len, int has_lead, uint64_t lead,

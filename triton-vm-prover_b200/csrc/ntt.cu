@@ -32,6 +32,8 @@
 //   K1 (lde_inv_a): inverse pass A, trace -> Y
 //   K2 (lde_mid):   inverse pass B, scale by N^-1 s_c^i, forward pass A -> Z_c
 //   K3 (lde_fwd_b): forward pass B for all cosets, written interleaved -> LDE
+#include <algorithm>
+
 #include "internal.cuh"
 #include "field.cuh"
 
@@ -915,16 +917,21 @@ cudaError_t launch_lde(const LdePlan& pl, const uint64_t* trace, uint64_t tld, u
     // four-step split N = n1 * n2 (K2 runs the n1-point transforms, K1 and K3
     // the n2-point ones); the default is the balanced split, the tuning knob
     // "lde_split_l1" picks another valid one
+    // (both factors at least 2^6, so that every pass kernel has at least one
+    // whole tile of sequences)
     int l1 = (l + 1) / 2;
-    if (const int ks = tuning_lde_split_l1(); ks >= 1 && ks <= 12 && l - ks >= 1 && l - ks <= 12) l1 = ks;
+    if (const int ks = tuning_lde_split_l1(); ks >= 6 && ks <= 12 && l - ks >= 6 && l - ks <= 12) l1 = ks;
+    // K3 holds one sequence of every coset per tile: with a large expansion a
+    // smaller n2 keeps that tile within shared memory (2^22 rows x 16)
+    while (l1 < 12 && ((size_t)(1u << (l - l1)) + spad_words(1 << (l - l1), le)) * 8 > 227 * 1024) l1++;
     const int l2 = l - l1;
     const int tile = tuning_ntt_tile_log();
     const uint64_t N = 1ull << l;
-    const int lT1 = fit_lT(choose_lT(l2, tile), l2, 1);
+    const int lT1 = std::min(fit_lT(choose_lT(l2, tile), l2, 1), l1);
     const size_t smem1 = words_bytes((1u << l2) + spad_words(1 << l2, lT1));
-    const int lT2 = fit_lT(choose_lT(l1, tile), l1, 2);
+    const int lT2 = std::min(fit_lT(choose_lT(l1, tile), l1, 2), l2);
     const size_t smem2 = words_bytes((size_t)(1u << l1) + 2 * spad_words(1 << l1, lT2));
-    const int lT3 = fit_lT(clampi(tile - l2 - le, 0, 1), l2, 1, le);
+    const int lT3 = std::min(fit_lT(clampi(tile - l2 - le, 0, 1), l2, 1, le), l1);
     const size_t smem3 = words_bytes((1u << l2) + spad_words(1 << l2, lT3 + le));
     uint64_t* Y = scratch;
     for (uint64_t c0 = 0; c0 < cols; c0 += 65535) {

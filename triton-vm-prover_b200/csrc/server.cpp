@@ -98,6 +98,7 @@ struct tvmc_server {
     std::condition_variable cv;  // queue changes, completions, releases
     std::deque<Request*> queue_small, queue_large;
     int max_large = 1, large_running = 0;
+    bool group_small = true;  // queued small requests are committed together (tvmc_commit_multi)
     std::unordered_map<uint64_t, std::unique_ptr<Request>> reqs;
     size_t used = 0, peak = 0;
     uint64_t next_id = 1, submitted = 0, completed = 0, failed = 0, released = 0;
@@ -110,23 +111,34 @@ namespace {
 
 struct DoneCtx {
     tvmc_server* s;
-    Request* r;
+    std::vector<Request*> rs;  // one request, or a group committed together
 };
 
 void CUDART_CB on_done(void* p) {
     std::unique_ptr<DoneCtx> ctx(static_cast<DoneCtx*>(p));
     tvmc_server* s = ctx->s;
     std::lock_guard<std::mutex> lk(s->mu);
-    Request* r = ctx->r;
-    r->state = State::Done;
-    r->t_done = now_ns();
-    s->used -= r->transient;
-    s->inflight[r->stream]--;
-    s->running--;
-    if (r->large) s->large_running--;
-    s->completed++;
+    const uint64_t t = now_ns();
+    for (Request* r : ctx->rs) {
+        r->state = State::Done;
+        r->t_done = t;
+        s->used -= r->transient;
+        s->inflight[r->stream]--;
+        s->running--;
+        if (r->large) s->large_running--;
+        s->completed++;
+    }
     s->cv.notify_all();
 }
+
+// A small request joins a multi-table group (tvmc_commit_multi) when it is a
+// plain commitment of a column-major trace.
+bool groupable(const Request* r) {
+    return !r->large && r->R == 0 && r->trace_offset % 0xFFFFFFFF00000001ull == 1 &&
+           !(r->flags & (TVMC_TRACE_ROW_MAJOR | TVMC_FRUGAL | TVMC_RAND_TRUNCATE));
+}
+constexpr size_t GROUP_MAX_TABLES = 64;
+constexpr size_t GROUP_MAX_TRACE_WORDS = size_t(1) << 25;  // 256 MB of traces per group
 
 void fail_request(tvmc_server* s, Request* r, int status, const std::string& msg) {
     r->state = State::Failed;
@@ -151,6 +163,60 @@ Request* pick(tvmc_server* s) {
     return nullptr;
 }
 
+// Issues a group of admitted small requests (lock held on entry and exit) as
+// one tvmc_commit_multi on the least-loaded small-table stream: their row
+// hashes run as one launch, so queued small tables fill the GPU together.
+void issue_group(tvmc_server* s, std::vector<Request*>& g, std::unique_lock<std::mutex>& lk) {
+    int best = 0;
+    for (int i = 0; i < s->n_small; i++)
+        if (s->inflight[i] < s->inflight[best]) best = i;
+    const uint64_t t0 = now_ns();
+    std::vector<tvmc_multi_table> tabs;
+    for (Request* r : g) {
+        s->used += r->resident + r->transient;
+        r->stream = best;
+        s->inflight[best]++;
+        s->running++;
+        r->state = State::Running;
+        r->t_start = t0;
+        tabs.push_back(tvmc_multi_table{r->trace, r->n, r->width, r->expansion, r->offset});
+    }
+    s->peak = std::max(s->peak, s->used);
+    const uint32_t flags = (g[0]->flags & TVMC_TRACE_DEVICE) | (s->keep_lde ? 0u : (uint32_t)TVMC_DISCARD_LDE);
+    cudaStream_t st = s->streams[best];
+    lk.unlock();
+    std::vector<tvmc_commitment*> cs(g.size(), nullptr);
+    int rc = tvmc_commit_multi(tabs.data(), tabs.size(), flags, st, cs.data());
+    const std::string err = rc ? tvmc_last_error() : "";
+    DoneCtx* ctx = nullptr;
+    if (!rc) {
+        ctx = new DoneCtx{s, g};
+        lk.lock();
+        for (size_t i = 0; i < g.size(); i++) g[i]->c = cs[i];  // set before the callback can run
+        lk.unlock();
+        if (cudaLaunchHostFunc(st, on_done, ctx) != cudaSuccess) {
+            delete ctx;
+            ctx = nullptr;
+            rc = TVMC_ERR_CUDA;
+        }
+    }
+    lk.lock();
+    if (!ctx) {
+        for (size_t i = 0; i < g.size(); i++) {
+            Request* r = g[i];
+            s->used -= r->resident + r->transient;
+            s->inflight[best]--;
+            s->running--;
+            r->c = nullptr;
+            fail_request(s, r, rc, rc == TVMC_ERR_CUDA && err.empty() ? "cannot queue the completion callback" : err);
+        }
+        lk.unlock();
+        for (auto* c : cs)
+            if (c) tvmc_commitment_free(c);
+        lk.lock();
+    }
+}
+
 void dispatch_loop(tvmc_server* s) {
     cudaSetDevice(s->device);
     std::unique_lock<std::mutex> lk(s->mu);
@@ -162,6 +228,27 @@ void dispatch_loop(tvmc_server* s) {
         const size_t need = r->resident + r->transient;
         if (need > s->budget) {
             fail_request(s, r, TVMC_ERR_NOMEM, "request footprint exceeds the server's HBM budget");
+            continue;
+        }
+        if (s->group_small && groupable(r)) {
+            // continuous batching: every queued small request that can join, in
+            // arrival order, while the budget holds
+            std::vector<Request*> g{r};
+            size_t words = r->n * r->width, extra = need;
+            for (auto it = s->queue_small.begin(); it != s->queue_small.end() && g.size() < GROUP_MAX_TABLES;) {
+                Request* q = *it;
+                const size_t qn = q->resident + q->transient;
+                if (!groupable(q) || (q->flags & TVMC_TRACE_DEVICE) != (r->flags & TVMC_TRACE_DEVICE) ||
+                    words + q->n * q->width > GROUP_MAX_TRACE_WORDS || s->used + extra + qn > s->budget) {
+                    ++it;
+                    continue;
+                }
+                g.push_back(q);
+                words += q->n * q->width;
+                extra += qn;
+                it = s->queue_small.erase(it);
+            }
+            issue_group(s, g, lk);
             continue;
         }
         s->used += need;
@@ -199,7 +286,7 @@ void dispatch_loop(tvmc_server* s) {
         }
         r->c = c;  // set before the completion callback can run
         lk.unlock();
-        auto* ctx = new DoneCtx{s, r};
+        auto* ctx = new DoneCtx{s, {r}};
         const cudaError_t e = cudaLaunchHostFunc(st, on_done, ctx);
         lk.lock();
         if (e != cudaSuccess) {
@@ -230,13 +317,15 @@ int tvmc_server_create(const tvmc_server_config* cfg, tvmc_server** out) {
     *out = nullptr;
     tvmc_server_config c{};
     if (cfg) c = *cfg;
-    if (c.flags & ~(uint32_t)TVMC_SERVER_KEEP_LDE) return tvmc::set_error(TVMC_ERR_INVALID, "unknown server flags");
+    if (c.flags & ~(uint32_t)(TVMC_SERVER_KEEP_LDE | TVMC_SERVER_NO_GROUPING))
+        return tvmc::set_error(TVMC_ERR_INVALID, "unknown server flags");
     auto s = std::make_unique<tvmc_server>();
     if (cudaGetDevice(&s->device) != cudaSuccess) return tvmc::set_error(TVMC_ERR_CUDA, "no CUDA device");
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return tvmc::set_error(TVMC_ERR_CUDA, "cudaMemGetInfo");
     s->budget = c.hbm_budget_bytes ? c.hbm_budget_bytes : free_b / 10 * 9;
     s->keep_lde = c.flags & TVMC_SERVER_KEEP_LDE;
+    s->group_small = !(c.flags & TVMC_SERVER_NO_GROUPING);
     s->max_large = c.max_large_inflight ? (int)c.max_large_inflight : 2;
     long long sb = 0;
     if (tvmc_get_tuning("lde_scratch_bytes", &sb) == TVMC_OK && sb > 0) s->scratch_budget = (size_t)sb;

@@ -62,13 +62,24 @@ __device__ __constant__ T5RoundBias c_t5_bias = t5_round_bias();
 // input byte v, in lane l's private column.
 constexpr int T5_SBOX_WORDS = 256 * 32;
 
-// Fill the lane-replicated byte table; call from all threads, then sync.
-__device__ __forceinline__ void t5_sbox_init(uint32_t* tbl) {
-    for (int i = threadIdx.x; i < T5_SBOX_WORDS; i += blockDim.x) {
-        const int x = (i >> 5) + 1;
-        const int c = (x * x % 257) * x % 257;
-        tbl[i] = (uint32_t)((c + 256) % 257);
+// The byte table itself, generated at compile time: v -> (v + 1)^3 - 1 over F_257.
+struct T5Sbox {
+    uint32_t v[256];
+};
+constexpr T5Sbox t5_sbox_bytes() {
+    T5Sbox t{};
+    for (int v = 0; v < 256; v++) {
+        const int x = v + 1;
+        t.v[v] = (uint32_t)(((x * x % 257) * x % 257 + 256) % 257);
     }
+    return t;
+}
+__device__ __constant__ T5Sbox c_t5_sbox = t5_sbox_bytes();
+
+// Fill the lane-replicated byte table from the constant bank (all 32 lanes of
+// a warp read the same entry); call from all threads, then sync.
+__device__ __forceinline__ void t5_sbox_init(uint32_t* tbl) {
+    for (int i = threadIdx.x; i < T5_SBOX_WORDS; i += blockDim.x) tbl[i] = c_t5_sbox.v[i >> 5];
 }
 
 // Byte-wise S-box of a 32-bit word through the lane's private table column:

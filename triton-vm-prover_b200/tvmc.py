@@ -137,6 +137,7 @@ SIGNATURES = {
     "tvmc_server_release": (ctypes.c_int, [_vp, ctypes.c_uint64]),
     "tvmc_server_get_stats": (ctypes.c_int, [_vp, _vp]),
     "tvmc_server_destroy": (ctypes.c_int, [_vp]),
+    "tvmc_commit_multi": (ctypes.c_int, [_vp, _sz, ctypes.c_uint32, _vp, _vp]),
     "tvmc_set_tuning": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_longlong]),
     "tvmc_get_tuning": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_longlong)]),
 }
@@ -367,6 +368,39 @@ def merkle_root_gpu(d_leaves: int, d_root: int, n: int, stream=None) -> None:
 
 
 # ---------------------------------------------------------------- commitment
+
+class MultiTable(ctypes.Structure):
+    _fields_ = [("trace", ctypes.c_void_p), ("trace_len", ctypes.c_size_t), ("width", ctypes.c_size_t),
+                ("expansion", ctypes.c_uint32), ("offset", ctypes.c_uint64)]
+
+
+def commit_multi(traces, expansion: int = 4, offset: int = 7, device_ptr: bool = False, shapes=None,
+                 discard_lde: bool = False, stream=None, sync: bool = False) -> list:
+    """tvmc_commit_multi: several plain commitments with one multi-table row
+    hash.  traces: host (width, n) arrays, or with device_ptr=True device
+    pointers with shapes = [(n, width), ...]."""
+    descs, keep = [], []
+    for i, t in enumerate(traces):
+        if device_ptr:
+            n, w = shapes[i]
+            ptr = int(t)
+        else:
+            a = _u64(t)
+            w, n = a.shape
+            keep.append(a)
+            ptr = a.ctypes.data if a.size else None
+        descs.append(MultiTable(ptr, n, w, expansion, offset))
+    arr = (MultiTable * max(1, len(descs)))(*descs)
+    hs = (_vp * max(1, len(descs)))()
+    flags = (TRACE_DEVICE if device_ptr else 0) | (DISCARD_LDE if discard_lde else 0) | (SYNC if sync else 0)
+    _check(lib().tvmc_commit_multi(ctypes.cast(arr, _vp), len(descs), flags, _stream(stream), ctypes.cast(hs, _vp)))
+    out = []
+    for d, h in zip(descs, hs[:len(descs)]):
+        c = Commitment._wrap(_vp(h), d.width, d.trace_len * expansion, keep)
+        c.trace_len = d.trace_len
+        out.append(c)
+    return out
+
 
 class Commitment:
     """A committed table: device-resident LDE (column-major) and heap tree.
@@ -627,6 +661,7 @@ class Batch:
 
 
 SERVER_KEEP_LDE = 0x1
+SERVER_NO_GROUPING = 0x2
 
 
 class ServerConfig(ctypes.Structure):
@@ -645,8 +680,10 @@ class Server:
     dispatched over worker streams as they arrive, trees kept on the device
     for openings until release."""
 
-    def __init__(self, hbm_budget_bytes: int = 0, streams: int = 4, keep_lde: bool = False, max_large: int = 0):
-        cfg = ServerConfig(hbm_budget_bytes, streams, SERVER_KEEP_LDE if keep_lde else 0, max_large)
+    def __init__(self, hbm_budget_bytes: int = 0, streams: int = 4, keep_lde: bool = False, max_large: int = 0,
+                 group_small: bool = True):
+        flags = (SERVER_KEEP_LDE if keep_lde else 0) | (0 if group_small else SERVER_NO_GROUPING)
+        cfg = ServerConfig(hbm_budget_bytes, streams, flags, max_large)
         h = _vp()
         _check(lib().tvmc_server_create(ctypes.byref(cfg), ctypes.byref(h)))
         self.h = h
