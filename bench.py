@@ -596,6 +596,46 @@ def run_ours(args):
                "pipelined": "step k+1 issued before step k's roots are read",
                "ms_per_step": 1e3 * te / args.steps}
 
+        # the same from row-major host traces (the reference CPU layout,
+        # vector<vector<BFE>>): upload, device transpose, LDE, hash, tree
+        if not args.skip_row_major:
+            rm = {}
+            for w, hc in ((W_MAIN, h_main), (W_AUX, h_aux)):
+                r = torch.empty((n, w), dtype=torch.int64, pin_memory=True)
+                r.copy_(hc.t())
+                rm[w] = r.numpy().view(np.uint64)
+
+            def run_rm(steps):
+                for _ in range(steps):
+                    a = tvmc.Commitment(rm[W_MAIN], row_major=True, stream=sp, expansion=EXPANSION,
+                                        offset=OFFSET, discard_lde=True)
+                    b = tvmc.Commitment(rm[W_AUX], row_major=True, stream=sp_e2e, expansion=EXPANSION,
+                                        offset=OFFSET, discard_lde=True)
+                    a.root()
+                    b.root()
+                    a.free()
+                    b.free()
+
+            run_rm(max(1, args.warmup // 2))
+            torch.cuda.synchronize()
+            barrier()
+            t0 = time.perf_counter()
+            run_rm(args.steps)
+            torch.cuda.synchronize()
+            trm = max_over_ranks(time.perf_counter() - t0, dev)
+            e2e["row_major"] = {"value": whole_job_rate(cells_step * args.steps, ws, trm), "unit": "cells/s",
+                                "ms_per_step": 1e3 * trm / args.steps,
+                                "transpose": "TMA tiles" if tvmc.get_tuning("transpose_tma") == 1
+                                else "shared-memory tiles",
+                                "what": "row-major pinned host traces (the reference CPU layout): upload, "
+                                        "device transpose, LDE, row hash, tree; roots read back; not pipelined"}
+            del rm
+
+    # serving figures (BASELINE's metric names serving p50/p99 beside throughput)
+    serving = None
+    if rank == 0 and ws == 1 and not args.skip_serving and args.log_n == LOG_N:
+        serving = serving_compact(torch, dev, h_main if e2e else None, h_aux if e2e else None)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.skip_cpu:
         v, cores, sample, detail = cpu_reference_sample(args.log_n)
@@ -634,6 +674,7 @@ def run_ours(args):
                              "ms_per_step": sum(lde_ms) / args.steps,
                              "ms_per_table_min_max": [min(lde_ms), max(lde_ms)]},
             "e2e": e2e,
+            "serving": serving,
             "cpu_baseline": cpu,
             "clocks": clocks,
             "gpu_launches": launches,
@@ -757,112 +798,199 @@ def run_frugal(args):
     print(json.dumps(line), flush=True)
 
 
-def run_serving(args):
-    """Poisson arrivals, mixed sizes, 80 openings per request: serving loop vs
-    the plain per-request drop-in (one commit at a time, in arrival order)."""
-    import threading
-    import torch
-    import tvmc
-    dev = torch.device("cuda", 0)
-    torch.cuda.set_device(dev)
-    rng = np.random.default_rng(0x7E5EED05)
-    M = args.requests
-    shapes = _seeded_shapes(0x7E5EED05, M, 10, args.serve_max_log_n)
-    host = {}
-    for (n, w) in sorted(set(shapes)):  # one pinned host table per shape class
-        d = random_trace(torch, w, n, 5000 + n + w, dev)
-        h = torch.empty((w, n), dtype=torch.int64, pin_memory=True)
-        h.copy_(d)
-        host[(n, w)] = h
-        del d
-    torch.cuda.synchronize()
-    torch.cuda.empty_cache()
-    reqs = [host[sh].numpy().view(np.uint64) for sh in shapes]
-    opens = [rng.integers(0, EXPANSION * n, 80) for n, _ in shapes]
-    cells = [EXPANSION * n * w for n, w in shapes]
-    st = torch.cuda.Stream(dev)
+class ServingStream:
+    """The serving workload: Poisson arrivals of commitment requests with
+    heights 2^10 .. 2^max_log log-uniform and widths 379 / 264 limbs by seed,
+    80 openings each.  Request traces are prefixes of two pinned host tables
+    (one per width), so every request is a contiguous column-major host trace.
 
-    def plain(arr_ns):
+    plain(): the per-request drop-in -- one tvmc_commit at a time in arrival
+    order, root read back, then the openings.  served(): the serving loop.
+    ceiling(): per shape class the GPU time of a commit with the trace already
+    on the device and the time of the trace's host-to-device copy alone; no
+    scheduler can exceed M / max(sum of GPU times, sum of copy times)."""
+
+    def __init__(self, torch, dev, M, max_log, seed, h_main=None, h_aux=None):
+        self.torch, self.dev, self.M = torch, dev, M
+        self.shapes = _seeded_shapes(seed, M, 10, max_log)
+        n_max = max(n for n, _ in self.shapes)
+        host, self.host_t = {}, {}
+        for w, h in ((W_MAIN, h_main), (W_AUX, h_aux)):
+            if h is None or h.shape[0] != w or h.shape[1] < n_max:
+                d = random_trace(torch, w, n_max, 5000 + w, dev)
+                h = torch.empty((w, n_max), dtype=torch.int64, pin_memory=True)
+                h.copy_(d)
+                del d
+            self.host_t[w] = h.reshape(-1)  # pinned; request traces are its prefixes
+            host[w] = h.numpy().view(np.uint64).reshape(-1)
+        torch.cuda.synchronize()
+        self.reqs = [host[w][: w * n].reshape(w, n) for n, w in self.shapes]
+        rng = np.random.default_rng(seed + 1)
+        self.opens = [rng.integers(0, EXPANSION * n, 80) for n, _ in self.shapes]
+        self.cells = [EXPANSION * n * w for n, w in self.shapes]
+        self.large = np.array([c * 8 > (128 << 20) for c in self.cells])
+        self.stream = torch.cuda.Stream(dev)
+
+    @staticmethod
+    def _wait_until(target):
+        while time.monotonic_ns() < target:
+            time.sleep(max(0.0, (target - time.monotonic_ns()) / 1e9 - 0.0005))
+
+    def plain(self, arr_ns):
+        import tvmc
         lat, svc = [], []
         t0 = time.monotonic_ns() + 20_000_000
-        for i, t in enumerate(reqs):
+        for i, t in enumerate(self.reqs):
             target = t0 + arr_ns[i]
-            while time.monotonic_ns() < target:
-                time.sleep(max(0.0, (target - time.monotonic_ns()) / 1e9 - 0.0005))
+            self._wait_until(target)
             start = time.monotonic_ns()
-            c = tvmc.Commitment(t, stream=st.cuda_stream, discard_lde=True)
+            c = tvmc.Commitment(t, stream=self.stream.cuda_stream, discard_lde=True)
             c.root()
             done = time.monotonic_ns()
             lat.append(done - target)
             svc.append(done - start)
-            c.auth_paths(opens[i])
+            c.auth_paths(self.opens[i])
             c.free()
         return lat, (time.monotonic_ns() - t0 - arr_ns[0]) / 1e9, svc
 
-    def served(arr_ns):
+    def served(self, arr_ns, streams=4, max_large=0, group_small=False):
+        import threading
+        import tvmc
+        M = self.M
         lat, svc = [0] * M, [0] * M
         ids = [None] * M
         ready = [threading.Event() for _ in range(M)]
         t0 = time.monotonic_ns() + 20_000_000
-        with tvmc.Server(streams=args.serve_streams, max_large=args.serve_max_large) as srv:
+        with tvmc.Server(streams=streams, max_large=max_large, group_small=group_small) as srv:
             def waiter():
                 for i in range(M):
                     ready[i].wait()
                     srv.wait(ids[i])
-                    srv.open(ids[i], opens[i])
+                    srv.open(ids[i], self.opens[i])
                     _sub, start, done = srv.times(ids[i])
                     lat[i] = done - (t0 + arr_ns[i])
                     svc[i] = done - start
                     srv.release(ids[i])
             th = threading.Thread(target=waiter)
             th.start()
-            for i, t in enumerate(reqs):
-                target = t0 + arr_ns[i]
-                while time.monotonic_ns() < target:
-                    time.sleep(max(0.0, (target - time.monotonic_ns()) / 1e9 - 0.0005))
+            for i, t in enumerate(self.reqs):
+                self._wait_until(t0 + arr_ns[i])
                 ids[i] = srv.submit(t)
                 ready[i].set()
             th.join()
             stats = srv.stats()
         return lat, (time.monotonic_ns() - t0 - arr_ns[0]) / 1e9, stats, svc
 
-    large = np.array([c * 8 > (128 << 20) for c in cells])
-
-    def summ(lat, span, svc):
+    def summary(self, lat, span, svc):
         ms = np.array(lat) / 1e6
         sv = np.array(svc) / 1e6
         out = {"p50_ms": float(np.percentile(ms, 50)), "p99_ms": float(np.percentile(ms, 99)),
-               "mean_ms": float(ms.mean()), "throughput_rps": M / span, "cells_per_s": sum(cells) / span}
-        for name, sel in (("small", ~large), ("large", large)):
+               "mean_ms": float(ms.mean()), "throughput_rps": self.M / span, "cells_per_s": sum(self.cells) / span}
+        for name, sel in (("small", ~self.large), ("large", self.large)):
             if sel.any():
                 out[f"{name}_p50_ms"] = float(np.percentile(ms[sel], 50))
                 out[f"{name}_p99_ms"] = float(np.percentile(ms[sel], 99))
                 out[f"{name}_service_mean_ms"] = float(sv[sel].mean())
         return out
 
+    def arrivals(self, rho, service_s):
+        lam = rho / service_s
+        gaps = np.random.default_rng(int(rho * 1000)).exponential(1.0 / lam, self.M)
+        return lam, [int(x) for x in (np.cumsum(gaps) - gaps[0]) * 1e9]
+
+    def ceiling(self, span_plain):
+        """GPU-only and copy-only time of the stream (CUDA events, per shape
+        class, median of 3), against the plain path's back-to-back span."""
+        import tvmc
+        torch = self.torch
+        gpu_ms, copy_ms = {}, {}
+        st = self.stream
+        for (n, w) in sorted(set(self.shapes)):
+            d = torch.empty(w * n, dtype=torch.int64, device=self.dev)
+            ht = self.host_t[w][: w * n]
+            g, cp = [], []
+            for k in range(4):
+                e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+                with torch.cuda.stream(st):
+                    e[0].record(st)
+                    d.copy_(ht, non_blocking=True)
+                    e[1].record(st)
+                    e[2].record(st)
+                    c = tvmc.Commitment(d.data_ptr(), width=w, trace_len=n, device_ptr=True,
+                                        stream=st.cuda_stream, discard_lde=True)
+                    e[3].record(st)
+                st.synchronize()
+                c.free()
+                if k:
+                    cp.append(e[0].elapsed_time(e[1]))
+                    g.append(e[2].elapsed_time(e[3]))
+            gpu_ms[(n, w)] = statistics.median(g)
+            copy_ms[(n, w)] = statistics.median(cp)
+            del d
+        sum_gpu = sum(gpu_ms[s] for s in self.shapes) / 1e3
+        sum_copy = sum(copy_ms[s] for s in self.shapes) / 1e3
+        bound = max(sum_gpu, sum_copy)
+        return {"gpu_busy_s": sum_gpu, "copy_s": sum_copy, "plain_span_s": span_plain,
+                "plain_gpu_busy_frac": sum_gpu / span_plain, "plain_copy_frac": sum_copy / span_plain,
+                "ceiling_rps": self.M / bound, "ceiling_vs_plain": span_plain / bound,
+                "bound_by": "gpu" if sum_gpu >= sum_copy else "host-to-device copies"}
+
+
+def serving_compact(torch, dev, h_main, h_aux, M=200, rho=1.5):
+    """The serving figures for the default bench line: one offered load, plain
+    vs served, plus the ceiling."""
+    ss = ServingStream(torch, dev, M, LOG_N, 0x7E5EED05, h_main, h_aux)
+    ss.plain([0] * M)  # warm-up: twiddle tables, pool, pinned paths
+    ss.served([0] * M)
+    lat0, span0, _ = ss.plain([0] * M)
+    ceil = ss.ceiling(span0)
+    lam, arr = ss.arrivals(rho, span0 / M)
+    pl = ss.summary(*ss.plain(arr))
+    sv_lat, sv_span, _, sv_svc = ss.served(arr)
+    sv = ss.summary(sv_lat, sv_span, sv_svc)
+    return {"requests": M, "load_vs_plain_capacity": rho, "rate_rps": lam,
+            "plain": {k: pl[k] for k in ("p50_ms", "p99_ms", "throughput_rps")},
+            "server": {k: sv[k] for k in ("p50_ms", "p99_ms", "throughput_rps")},
+            "throughput_vs_plain": sv["throughput_rps"] / pl["throughput_rps"],
+            "ceiling_vs_plain": ceil["ceiling_vs_plain"], "plain_gpu_busy_frac": ceil["plain_gpu_busy_frac"],
+            "plain_copy_frac": ceil["plain_copy_frac"],
+            "mix": f"heights 2^10..2^{LOG_N} log-uniform, widths 379/264, 80 openings each, pinned host traces"}
+
+
+def run_serving(args):
+    """Poisson arrivals, mixed sizes, 80 openings per request: serving loop vs
+    the plain per-request drop-in (one commit at a time, in arrival order),
+    swept over offered loads, with the ceiling any scheduler could reach."""
+    import torch
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    M = args.requests
+    ss = ServingStream(torch, dev, M, args.serve_max_log_n, 0x7E5EED05)
     zero = [0] * M
-    plain(zero)  # warm-up: twiddle tables, pool, pinned paths
-    served(zero)
-    lat0, span0, _ = plain(zero)  # back-to-back: the plain path's service time
+    ss.plain(zero)  # warm-up: twiddle tables, pool, pinned paths
+    ss.served(zero, args.serve_streams, args.serve_max_large)
+    lat0, span0, _ = ss.plain(zero)  # back-to-back: the plain path's service time
     service_s = span0 / M
+    ceil = ss.ceiling(span0)
     rates = []
     for rho in args.serve_loads:
-        lam = rho / service_s
-        gaps = np.random.default_rng(int(rho * 1000)).exponential(1.0 / lam, M)
-        arr = (np.cumsum(gaps) - gaps[0]) * 1e9
-        arr_ns = [int(x) for x in arr]
-        pl, pspan, psvc = plain(arr_ns)
-        sv, sspan, stats, ssvc = served(arr_ns)
-        rates.append({"load_vs_plain_capacity": rho, "rate_rps": lam, "plain": summ(pl, pspan, psvc),
-                      "server": summ(sv, sspan, ssvc), "server_peak_bytes": stats["bytes_peak"],
-                      "server_budget_bytes": stats["budget"]})
+        lam, arr_ns = ss.arrivals(rho, service_s)
+        pl, pspan, psvc = ss.plain(arr_ns)
+        sv, sspan, stats, ssvc = ss.served(arr_ns, args.serve_streams, args.serve_max_large)
+        entry = {"load_vs_plain_capacity": rho, "rate_rps": lam, "plain": ss.summary(pl, pspan, psvc),
+                 "server": ss.summary(sv, sspan, ssvc), "server_peak_bytes": stats["bytes_peak"],
+                 "server_budget_bytes": stats["budget"]}
+        if args.serve_grouped:
+            gp, gspan, _, gsvc = ss.served(arr_ns, args.serve_streams, args.serve_max_large, group_small=True)
+            entry["server_grouped"] = ss.summary(gp, gspan, gsvc)
+        rates.append(entry)
     line = {"metric": "serving latency p50/p99 and throughput", "workload": "serving", "requests": M,
-            "plain_service_ms_mean": 1e3 * service_s,
+            "plain_service_ms_mean": 1e3 * service_s, "ceiling": ceil,
             "config": {"heights": f"2^10..2^{args.serve_max_log_n} log-uniform", "widths": [W_MAIN, W_AUX],
                        "expansion": EXPANSION, "openings_per_request": 80, "server_streams": args.serve_streams,
                        "server_max_large_inflight": args.serve_max_large,
                        "small_large_split": "LDE <= 128 MB is small",
-                       "host_buffers": "pinned, one per (height, width) class",
+                       "host_buffers": "pinned; each request a contiguous prefix of one of two tables",
                        "latency": "arrival -> root committed (server: completion callback time)"},
             "rates": rates, "n_gpus": 1, "data": "synthetic uniform field elements"}
     print(json.dumps(line), flush=True)
@@ -886,7 +1014,11 @@ def main():
                     help="with --impl reference: time the reference's own CUDA kernels (sm_100a build) instead")
     ap.add_argument("--ref-max-seconds", type=float, default=400.0,
                     help="reference arm: time budget for its full CPU steps")
-    ap.add_argument("--requests", type=int, default=48, help="serving: requests per rate")
+    ap.add_argument("--requests", type=int, default=500, help="serving: requests per rate")
+    ap.add_argument("--serve-grouped", action="store_true",
+                    help="serving: also run the server with small-request grouping on (TVMC_SERVER_GROUP_SMALL)")
+    ap.add_argument("--skip-serving", action="store_true", help="commit: no serving figures in the line")
+    ap.add_argument("--skip-row-major", action="store_true", help="commit: no row-major e2e case")
     ap.add_argument("--serve-streams", type=int, default=4)
     ap.add_argument("--serve-max-log-n", type=int, default=20)
     ap.add_argument("--serve-max-large", type=int, default=0,

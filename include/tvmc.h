@@ -79,6 +79,11 @@ int tvmc_evaluate_on_coset_gpu(const uint64_t* d_coeffs, size_t num_coeffs, size
 int tvmc_evaluate_on_coset_host(const uint64_t* coeffs, size_t num_coeffs, size_t num_cols, uint64_t* out,
                                 size_t domain_len, uint64_t offset);
 
+/* Row-major (the CPU layout vector<vector<BFE>>, d_in[r*cols + c]) to
+ * column-major (d_out[c*rows + r]) on the device, out of place.  Replaces
+ * qzc_rowmajor_to_colmajor_bfe (src/gpu/gpu_stark.cu:125-180). */
+int tvmc_rowmajor_to_colmajor_gpu(const uint64_t* d_in, size_t rows, size_t cols, uint64_t* d_out, void* stream);
+
 /* ---- LDE (include/gpu/kernels/lde_kernel.cuh lde_batch_gpu; src/ntt/ntt.cpp:121-131) ---- */
 
 /* Low-degree extension of num_columns column-major columns: interpolate each
@@ -203,6 +208,8 @@ typedef struct tvmc_commitment tvmc_commitment;
  *   "lde_scratch_bytes"   LDE intermediate budget per call (default 2 GiB); columns are
  *                         processed in chunks that fit
  *   "batch_streams"       worker streams a tvmc_batch spreads its tables over (default 8)
+ *   "transpose_tma"       1: row-major traces are transposed with TMA tile copies where the width
+ *                         and height are even; 2 (or 0, the default): shared-memory tiles
  *   "batch_multi_hash"    1: a tvmc_batch hashes all its tables with one multi-table launch after
  *                         their LDEs; 2: each worker stream hashes its own tables; default 1
  *   "lde_mid_ctas"        resident CTAs per SM for the fused LDE middle kernel: 2 (no register
@@ -368,10 +375,10 @@ int tvmc_batch_free(tvmc_batch* b);
  * running requests and the trees still held, and is issued at once on the
  * least-loaded of its worker streams.  Small tables (LDE up to 128 MB) run
  * concurrently on num_streams high-priority streams and never wait behind
- * large ones; plain small requests queued at the same time are committed
- * together as one tvmc_commit_multi (their row hashes share one launch, so a
- * burst of small tables fills the GPU instead of trickling through it) unless
- * TVMC_SERVER_NO_GROUPING is set; large tables, each enough to fill the GPU, go in arrival order
+ * large ones; with TVMC_SERVER_GROUP_SMALL, plain small requests queued at
+ * the same time are committed together as one tvmc_commit_multi (their row
+ * hashes share one launch, so a burst of small tables fills the GPU instead
+ * of trickling through it); large tables, each enough to fill the GPU, go in arrival order
  * onto one dedicated stream, with up to max_large_inflight of them issued at
  * once (the next one's upload overlaps the current one's kernels).  Each request's
  * Merkle tree stays on the device for openings until tvmc_server_release;
@@ -382,12 +389,12 @@ int tvmc_batch_free(tvmc_batch* b);
 typedef struct tvmc_server tvmc_server;
 
 #define TVMC_SERVER_KEEP_LDE 0x1u
-#define TVMC_SERVER_NO_GROUPING 0x2u /* commit every small request on its own */
+#define TVMC_SERVER_GROUP_SMALL 0x2u /* commit queued small requests together */
 
 typedef struct tvmc_server_config {
     size_t hbm_budget_bytes; /* 0: 90% of the device memory free at creation */
     uint32_t num_streams;    /* worker streams for small tables, 0: 4 (at most 64) */
-    uint32_t flags;          /* TVMC_SERVER_KEEP_LDE, TVMC_SERVER_NO_GROUPING */
+    uint32_t flags;          /* TVMC_SERVER_KEEP_LDE, TVMC_SERVER_GROUP_SMALL */
     uint32_t max_large_inflight; /* large tables issued at once, 0: 2 (at most 16) */
 } tvmc_server_config;
 

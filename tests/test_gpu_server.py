@@ -75,7 +75,7 @@ def test_server_groups_a_burst_of_small_requests(tv, oracle):
              for i, (l, w) in enumerate(zip(np.random.default_rng(5).integers(0, 9, 64),
                                             np.random.default_rng(6).choice([1, 9, 23, 379], 64)))]
     big = rand_u64(3199, (379, 1 << 18))
-    with tv.Server(streams=2) as srv:
+    with tv.Server(streams=2, group_small=True) as srv:
         rb = srv.submit(big)
         ids = [srv.submit(t) for t in small]
         for rid, t in zip(ids, small):

@@ -661,6 +661,8 @@ std::atomic<long long> g_tune_unfused_tree{0};
 std::atomic<long long> g_tune_mid_variant{0};
 int tvmc::tuning_lde_mid_ctas() { return g_tune_mid_ctas.load() == 3 ? 3 : 2; }
 int tvmc::tuning_lde_mid_variant() { return g_tune_mid_variant.load() == 2 ? 2 : 1; }
+std::atomic<long long> g_tune_transpose_tma{0};
+bool tvmc::tuning_transpose_tma() { return g_tune_transpose_tma.load() == 1; }
 std::atomic<long long> g_tune_split_l1{0};
 std::atomic<long long> g_tune_tile_log{0};
 int tvmc::tuning_lde_split_l1() { return (int)g_tune_split_l1.load(); }
@@ -803,6 +805,9 @@ int tvmc_set_tuning(const char* key, long long value) {
     } else if (!strcmp(key, "lde_mid_variant")) {
         if (value > 2) return fail(TVMC_ERR_INVALID, "lde_mid_variant must be 0, 1 or 2");
         g_tune_mid_variant = value;
+    } else if (!strcmp(key, "transpose_tma")) {
+        if (value > 2) return fail(TVMC_ERR_INVALID, "transpose_tma must be 0, 1 or 2");
+        g_tune_transpose_tma = value;
     } else if (!strcmp(key, "batch_multi_hash")) {
         if (value > 2) return fail(TVMC_ERR_INVALID, "batch_multi_hash must be 0, 1 or 2");
         g_tune_batch_multi = value;
@@ -828,6 +833,8 @@ int tvmc_get_tuning(const char* key, long long* value) {
     else if (!strcmp(key, "lde_mid_variant")) *value = g_tune_mid_variant;
     else if (!strcmp(key, "lde_split_l1")) *value = g_tune_split_l1;
     else if (!strcmp(key, "batch_multi_hash")) *value = g_tune_batch_multi;
+    else if (!strcmp(key, "transpose_tma")) *value = g_tune_transpose_tma;
+    else if (!strcmp(key, "tma_timeouts")) *value = (long long)tma_timeouts();
     else if (!strcmp(key, "ntt_tile_log")) *value = g_tune_tile_log;
     else if (!strcmp(key, "fail_alloc_after")) *value = g_fail_alloc_after;
     else if (!strcmp(key, "pool_used_bytes")) {
@@ -893,6 +900,13 @@ int tvmc_evaluate_on_coset_host(const uint64_t* coeffs, size_t num_coeffs, size_
     if (num_coeffs) CK(cudaMemcpy(a, coeffs, 8 * num_cols * num_coeffs, cudaMemcpyHostToDevice));
     if ((rc = tvmc_evaluate_on_coset_gpu(a, num_coeffs, num_cols, b, domain_len, offset, nullptr))) return rc;
     CK(cudaMemcpy(out, b, 8 * num_cols * domain_len, cudaMemcpyDeviceToHost));
+    return TVMC_OK;
+}
+
+int tvmc_rowmajor_to_colmajor_gpu(const uint64_t* d_in, size_t rows, size_t cols, uint64_t* d_out, void* stream) {
+    if ((rows && cols) && (!d_in || !d_out)) return fail(TVMC_ERR_INVALID, "null argument");
+    if (d_in == d_out && rows && cols) return fail(TVMC_ERR_INVALID, "the transpose is out of place");
+    CK(launch_transpose(d_in, cols, d_out, rows, rows, cols, as_stream(stream)));
     return TVMC_OK;
 }
 

@@ -180,6 +180,14 @@ cudaError_t launch_coset_scale(const uint64_t* in, uint64_t ild, uint64_t n, uin
 // Row-major (rows x cols, row stride rld) -> column-major (col stride cld).
 cudaError_t launch_transpose(const uint64_t* in, uint64_t rld, uint64_t* out, uint64_t cld, uint64_t rows,
                              uint64_t cols, cudaStream_t st);
+// The same with TMA tile copies (transpose.cu) for packed tables of even width
+// and height; cudaErrorNotSupported otherwise (the caller falls back).
+cudaError_t launch_transpose_tma(const uint64_t* in, uint64_t* out, uint64_t rows, uint64_t cols, cudaStream_t st);
+// TMA transpose tiles skipped because their load never completed (bounded wait).
+unsigned int tma_timeouts();
+// Tuning knob "transpose_tma": 1 = row-major -> column-major through TMA tiles
+// where the shape allows it, 2 = the shared-memory tile kernel always.
+bool tuning_transpose_tma();
 // Column-major -> row-major.
 cudaError_t launch_transpose_cm_to_rm(const uint64_t* in, uint64_t cld, uint64_t* out, uint64_t rld,
                                       uint64_t rows, uint64_t cols, cudaStream_t st);

@@ -1057,6 +1057,10 @@ __global__ void k_transpose(const uint64_t* __restrict__ in, uint64_t ild, uint6
 cudaError_t launch_transpose(const uint64_t* in, uint64_t rld, uint64_t* out, uint64_t cld, uint64_t rows,
                              uint64_t cols, cudaStream_t st) {
     if (rows == 0 || cols == 0) return cudaSuccess;
+    if (rld == cols && cld == rows && tuning_transpose_tma()) {
+        const cudaError_t e = launch_transpose_tma(in, out, rows, cols, st);
+        if (e != cudaErrorNotSupported) return e;  // odd sizes fall through to the tile kernel
+    }
     const dim3 g((unsigned)((cols + 31) / 32), (unsigned)((rows + 31) / 32));
     count_launch();
     k_transpose<<<g, dim3(32, 8), 0, st>>>(in, rld, out, cld, rows, cols);

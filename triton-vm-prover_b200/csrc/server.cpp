@@ -98,7 +98,7 @@ struct tvmc_server {
     std::condition_variable cv;  // queue changes, completions, releases
     std::deque<Request*> queue_small, queue_large;
     int max_large = 1, large_running = 0;
-    bool group_small = true;  // queued small requests are committed together (tvmc_commit_multi)
+    bool group_small = false;  // TVMC_SERVER_GROUP_SMALL: queued small requests committed together
     std::unordered_map<uint64_t, std::unique_ptr<Request>> reqs;
     size_t used = 0, peak = 0;
     uint64_t next_id = 1, submitted = 0, completed = 0, failed = 0, released = 0;
@@ -317,7 +317,7 @@ int tvmc_server_create(const tvmc_server_config* cfg, tvmc_server** out) {
     *out = nullptr;
     tvmc_server_config c{};
     if (cfg) c = *cfg;
-    if (c.flags & ~(uint32_t)(TVMC_SERVER_KEEP_LDE | TVMC_SERVER_NO_GROUPING))
+    if (c.flags & ~(uint32_t)(TVMC_SERVER_KEEP_LDE | TVMC_SERVER_GROUP_SMALL))
         return tvmc::set_error(TVMC_ERR_INVALID, "unknown server flags");
     auto s = std::make_unique<tvmc_server>();
     if (cudaGetDevice(&s->device) != cudaSuccess) return tvmc::set_error(TVMC_ERR_CUDA, "no CUDA device");
@@ -325,7 +325,7 @@ int tvmc_server_create(const tvmc_server_config* cfg, tvmc_server** out) {
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return tvmc::set_error(TVMC_ERR_CUDA, "cudaMemGetInfo");
     s->budget = c.hbm_budget_bytes ? c.hbm_budget_bytes : free_b / 10 * 9;
     s->keep_lde = c.flags & TVMC_SERVER_KEEP_LDE;
-    s->group_small = !(c.flags & TVMC_SERVER_NO_GROUPING);
+    s->group_small = c.flags & TVMC_SERVER_GROUP_SMALL;
     s->max_large = c.max_large_inflight ? (int)c.max_large_inflight : 2;
     long long sb = 0;
     if (tvmc_get_tuning("lde_scratch_bytes", &sb) == TVMC_OK && sb > 0) s->scratch_budget = (size_t)sb;

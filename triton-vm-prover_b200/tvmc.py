@@ -138,6 +138,7 @@ SIGNATURES = {
     "tvmc_server_get_stats": (ctypes.c_int, [_vp, _vp]),
     "tvmc_server_destroy": (ctypes.c_int, [_vp]),
     "tvmc_commit_multi": (ctypes.c_int, [_vp, _sz, ctypes.c_uint32, _vp, _vp]),
+    "tvmc_rowmajor_to_colmajor_gpu": (ctypes.c_int, [_vp, _sz, _sz, _vp, _vp]),
     "tvmc_set_tuning": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_longlong]),
     "tvmc_get_tuning": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_longlong)]),
 }
@@ -661,7 +662,7 @@ class Batch:
 
 
 SERVER_KEEP_LDE = 0x1
-SERVER_NO_GROUPING = 0x2
+SERVER_GROUP_SMALL = 0x2
 
 
 class ServerConfig(ctypes.Structure):
@@ -681,8 +682,8 @@ class Server:
     for openings until release."""
 
     def __init__(self, hbm_budget_bytes: int = 0, streams: int = 4, keep_lde: bool = False, max_large: int = 0,
-                 group_small: bool = True):
-        flags = (SERVER_KEEP_LDE if keep_lde else 0) | (0 if group_small else SERVER_NO_GROUPING)
+                 group_small: bool = False):
+        flags = (SERVER_KEEP_LDE if keep_lde else 0) | (SERVER_GROUP_SMALL if group_small else 0)
         cfg = ServerConfig(hbm_budget_bytes, streams, flags, max_large)
         h = _vp()
         _check(lib().tvmc_server_create(ctypes.byref(cfg), ctypes.byref(h)))
