@@ -213,10 +213,10 @@ typedef struct tvmc_commitment tvmc_commitment;
  *   "batch_multi_hash"    1: a tvmc_batch hashes all its tables with one multi-table launch after
  *                         their LDEs; 2: each worker stream hashes its own tables; default 1
  *   "lde_mid_ctas"        resident CTAs per SM for the fused LDE middle kernel: 2 (no register
- *                         spills) or 3 (a few spills); default 2
+ *                         spills) or 3 (a few spills); default 3
  *   "lde_mid_variant"     1: the fused LDE middle kernel reads its twiddles from global tables per
  *                         coset; 2: it forms the inter-pass twiddles once per CTA in shared
- *                         memory for all cosets; default 1
+ *                         memory for all cosets; default 2
  *   "lde_split_l1"        log2 of the LDE's four-step factor n1 (6 .. 12, with log2(N) - n1 also
  *                         in 6 .. 12, else the balanced split is used); default 0 = balanced
  *   "ntt_tile_log"        log2 of the words an NTT/LDE pass CTA moves per tile (11 .. 15);

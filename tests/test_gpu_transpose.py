@@ -20,7 +20,7 @@ def tma(tv):
 
 @pytest.mark.parametrize("mode", [1, 2])
 @pytest.mark.parametrize("rows,cols", [(1 << 20, 264), (1 << 12, 10), (64, 2), (2, 16), (32, 18), (96, 34),
-                                       (1 << 10, 379), (1 << 16, 1), (3, 5)])
+                                       (1 << 10, 379), (1 << 16, 1), (3, 5), (1 << 22, 3), (1 << 22, 2)])
 def test_transpose_equals_numpy(tma, rows, cols, mode):
     tv = tma
     tv.set_tuning("transpose_tma", mode)

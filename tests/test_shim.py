@@ -35,3 +35,32 @@ def test_shim_selftest_on_gpu():
     r = subprocess.run([BIN], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout[-4000:] + r.stderr[-2000:]
     assert " 0 failed" in r.stdout, r.stdout[-2000:]
+
+
+TC_BIN = os.path.join(ROOT, "tests", "cpp", "_bin", "table_commitment_check")
+
+
+def test_table_commitment_check_links_the_library():
+    if not os.path.exists(TC_BIN):
+        pytest.skip("TableCommitment check not built (needs the reference sources)")
+    out = subprocess.run(["ldd", TC_BIN], capture_output=True, text=True).stdout
+    assert "libtvmc.so" in out and "not found" not in out, out
+
+
+@pytest.mark.gpu
+def test_reference_table_commitment_over_the_drop_in():
+    """src/table/table_commitment.cpp, compiled unchanged, over the drop-in
+    layer: the per-column LDE of MasterMainTable::low_degree_extend, row
+    hashes, TableCommitment roots, paths, structures and verify vs the oracle."""
+    assert os.path.exists(TC_BIN), "tests/cpp/_bin/table_commitment_check missing: run __graft_entry__.build()"
+    r = subprocess.run([TC_BIN], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-4000:] + r.stderr[-2000:]
+    assert " 0 failed" in r.stdout, r.stdout[-2000:]
+
+
+@pytest.mark.gpu
+def test_per_column_drop_in_lde_equals_batched():
+    assert os.path.exists(TC_BIN)
+    r = subprocess.run([TC_BIN, "time", "12", "16"], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    assert '"equal": true' in r.stdout

@@ -29,11 +29,11 @@ int set_error(int code, const char* msg);
 // LDE entry point reports it.
 int check_lde_sizes(size_t trace_len, size_t extended_len, int* logn, int* le);
 // Tuning knob "lde_mid_ctas" (2 or 3 resident CTAs per SM for the fused LDE
-// middle kernel; default 2).
+// middle kernel; default 3).
 int tuning_lde_mid_ctas();
 // Tuning knob "lde_mid_variant": 1 = k_lde_mid_sym (twiddles from global tables
 // per coset), 2 = k_lde_mid_sym2 (inter-pass twiddles shared across cosets in
-// shared memory); 0 = the default.
+// shared memory); 0 = the default (2).
 int tuning_lde_mid_variant();
 // Tuning knob "lde_split_l1": log2 of the four-step factor n1 of the LDE (the
 // K2 transform size), 0 = balanced; a split with either factor outside

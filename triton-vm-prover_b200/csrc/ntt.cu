@@ -1061,10 +1061,17 @@ cudaError_t launch_transpose(const uint64_t* in, uint64_t rld, uint64_t* out, ui
         const cudaError_t e = launch_transpose_tma(in, out, rows, cols, st);
         if (e != cudaErrorNotSupported) return e;  // odd sizes fall through to the tile kernel
     }
-    const dim3 g((unsigned)((cols + 31) / 32), (unsigned)((rows + 31) / 32));
-    count_launch();
-    k_transpose<<<g, dim3(32, 8), 0, st>>>(in, rld, out, cld, rows, cols);
-    return cudaGetLastError();
+    // grid.y (row tiles) is limited to 65535: tall tables go in bands of rows
+    constexpr uint64_t BAND = 65535ull * 32;
+    for (uint64_t r0 = 0; r0 < rows; r0 += BAND) {
+        const uint64_t nr = rows - r0 < BAND ? rows - r0 : BAND;
+        const dim3 g((unsigned)((cols + 31) / 32), (unsigned)((nr + 31) / 32));
+        count_launch();
+        k_transpose<<<g, dim3(32, 8), 0, st>>>(in + r0 * rld, rld, out + r0, cld, nr, cols);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 cudaError_t launch_transpose_cm_to_rm(const uint64_t* in, uint64_t cld, uint64_t* out, uint64_t rld,
