@@ -546,7 +546,7 @@ def run_ours(args):
     # main-table launch (795.3 MB read + 14.8 MB written), scaled by rows
     traffic, traffic_src = None, None
     if W_MAIN == 379:
-        traffic = (795.3e6 + 14.8e6) * L / (1 << 18)
+        traffic = (795.35e6 + 14.95e6) * L / (1 << 18)
         traffic_src = "ncu dram__bytes_read+write of a 2^18x379 launch, scaled by LDE rows (main table)"
 
     # e2e: pinned host traces through the public C ABI, roots read back
