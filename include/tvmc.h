@@ -233,8 +233,10 @@ int tvmc_set_tuning(const char* key, long long value);
  * TVMC_DISCARD_LDE commitments per (device, stream) once used, and the device's
  * stream-ordered memory pool keeps freed memory, so that repeated commits never
  * wait for the driver to map memory.  This frees
- * that scratch and returns the pool's unused memory on the current device; it
- * synchronizes the device first. */
+ * that scratch, the cached twiddle and coset-scale tables (unless a tvmc_batch
+ * is alive on the device: its graph refers to them) and returns the pool's
+ * unused memory on the current device; it synchronizes the device first.  Call
+ * it only while no other thread is issuing work to this library on the device. */
 int tvmc_release_cached_memory(void);
 /* Frees the buffers this library keeps for one stream (and its upload stream),
  * ordered after the work already queued on it.  Call before destroying a

@@ -113,6 +113,7 @@ struct DevTables {
     std::map<int, std::pair<uint64_t*, uint64_t*>> wn_f, wn_i;                  // logn -> (lo, hi)
     std::map<std::tuple<int, int, uint64_t>, std::pair<uint64_t*, uint64_t*>> sc;  // (logn, le, offset)
     bool pool_set = false;
+    int live_batches = 0;  // batches hold plan pointers in their graphs: tables stay while any is alive
 };
 std::mutex g_mu;
 std::map<int, DevTables> g_dev;
@@ -518,8 +519,12 @@ int acc_stream(cudaStream_t* out) {
     CK(cudaGetDevice(&dev));
     auto it = t_acc.s.find(dev);
     if (it == t_acc.s.end()) {
+        // the greatest priority: an opening's small gather kernel is dispatched
+        // ahead of the remaining CTAs of the commits filling the GPU
+        int lo = 0, hi = 0;
+        CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
         cudaStream_t st;
-        CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, hi));
         it = t_acc.s.emplace(dev, st).first;
     }
     *out = it->second;
@@ -687,6 +692,7 @@ struct tvmc_batch {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     unsigned long long kernels_per_run = 0;
+    bool counted = false;  // holds a DevTables::live_batches count
 };
 
 namespace {
@@ -788,6 +794,25 @@ int tvmc_release_cached_memory(void) {
             } else {
                 ++it;
             }
+        }
+        // The twiddle and coset-scale tables: one set per (size, expansion, offset)
+        // ever used, so randomized LDEs with many distinct offsets would otherwise
+        // keep growing them.  They are rebuilt on the next use.
+        auto t = g_dev.find(dev);
+        if (t != g_dev.end() && t->second.live_batches == 0) {
+            DevTables& T = t->second;
+            for (auto* m : {&T.wn_f, &T.wn_i})
+                for (auto& kv : *m) {
+                    cudaFree(kv.second.first);
+                    cudaFree(kv.second.second);
+                }
+            for (auto& kv : T.sc) {
+                cudaFree(kv.second.first);
+                cudaFree(kv.second.second);
+            }
+            T.wn_f.clear();
+            T.wn_i.clear();
+            T.sc.clear();
         }
     }
     cudaMemPool_t pool;
@@ -1639,6 +1664,10 @@ int tvmc_commitment_free(tvmc_commitment* c) {
 
 int tvmc_batch_free(tvmc_batch* b) {
     if (!b) return TVMC_OK;
+    if (b->counted) {
+        std::lock_guard<std::mutex> lk(g_mu);
+        g_dev[b->device].live_batches--;
+    }
     for (auto* c : b->tables) destroy_commitment(c);
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
@@ -1671,6 +1700,11 @@ int tvmc_batch_create(const tvmc_table_shape* shapes, size_t count, tvmc_batch**
         return code;
     };
     CK(cudaGetDevice(&b->device));
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        g_dev[b->device].live_batches++;
+        b->counted = true;
+    }
     b->shapes.assign(shapes, shapes + count);
     const long long ks = g_tune_batch_streams.load();
     const size_t K = std::min<size_t>(count, ks > 0 ? (size_t)ks : 8);

@@ -334,9 +334,12 @@ int tvmc_server_create(const tvmc_server_config* cfg, tvmc_server** out) {
     const int ns = s->n_small + 1;  // small-table streams + the large-table stream
     int lo_prio = 0, hi_prio = 0;
     cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio);
+    // small tables one step below the greatest priority, which the openings'
+    // accessor streams use; large tables at the lowest
+    const int small_prio = hi_prio < lo_prio ? hi_prio + 1 : hi_prio;
     for (int i = 0; i < ns; i++) {
         cudaStream_t st;
-        const int prio = i < s->n_small ? hi_prio : lo_prio;
+        const int prio = i < s->n_small ? small_prio : lo_prio;
         if (cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, prio) != cudaSuccess) {
             for (auto x : s->streams) cudaStreamDestroy(x);
             return tvmc::set_error(TVMC_ERR_CUDA, "cannot create worker streams");
