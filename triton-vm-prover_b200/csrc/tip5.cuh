@@ -220,6 +220,36 @@ __device__ __forceinline__ double t5_half_biased(uint32_t v) {
     return __hiloint2double(0x43300000, (int)v);
 }
 
+// lo + hi*2^32 (mod p) from the two biased MDS halves 2^52 + lo and 2^52 + hi
+// (lo, hi < 2^52), as 32-bit limbs: with lo = L1*2^32 + L0 and hi = H1*2^32 + H0
+// (L1, H1 < 2^20), lo + hi*2^32 = L0 + (L1 + H0)*2^32 + H1*2^64, and
+// 2^64 = 2^32 - 1 (mod p) turns it into L0 - H1 + (H0 + L1 + H1)*2^32.  The
+// carry c of the high sum and the borrows of the subtraction net to c in
+// {-1, 0, 1}, folded back as c*(2^32 - 1): for c = 1 the high limb is below
+// 2^21, for c = -1 it is 2^32 - 1, so the fold cannot wrap.  The low limbs of the
+// doubles are L0 and H0 as they are; only the high limbs need masking.
+__device__ __forceinline__ uint64_t t5_recombine(double dlo, double dhi) {
+    const uint32_t l0 = (uint32_t)__double2loint(dlo), l1 = (uint32_t)__double2hiint(dlo) & 0xFFFFFu;
+    const uint32_t h0 = (uint32_t)__double2loint(dhi), h1 = (uint32_t)__double2hiint(dhi) & 0xFFFFFu;
+    uint32_t x0, x1;
+    asm("{\n\t"
+        ".reg .u32 a, c, e0, e1;\n\t"
+        "add.u32 a, %3, %5;\n\t"
+        "add.cc.u32 %1, %4, a;\n\t"
+        "addc.u32 c, 0, 0;\n\t"
+        "sub.cc.u32 %0, %2, %5;\n\t"
+        "subc.cc.u32 %1, %1, 0;\n\t"
+        "subc.u32 c, c, 0;\n\t"
+        "neg.s32 e0, c;\n\t"
+        "shr.s32 e1, c, 31;\n\t"
+        "add.cc.u32 %0, %0, e0;\n\t"
+        "addc.u32 %1, %1, e1;\n\t"
+        "}"
+        : "=r"(x0), "=r"(x1)
+        : "r"(l0), "r"(l1), "r"(h0), "r"(h1));
+    return ((uint64_t)x1 << 32) | x0;
+}
+
 // MDS of the state plus the round constants of round rnd.
 __device__ __forceinline__ void t5_mds(uint64_t s[T5_STATE], int rnd) {
     double dl[T5_STATE], dh[T5_STATE];
@@ -231,17 +261,7 @@ __device__ __forceinline__ void t5_mds(uint64_t s[T5_STATE], int rnd) {
     t5_mds_half(dl, c_t5_bias.lo + rnd * T5_STATE);
     t5_mds_half(dh, c_t5_bias.hi + rnd * T5_STATE);
 #pragma unroll
-    for (int r = 0; r < T5_STATE; r++) {
-        const uint64_t lo = (uint64_t)__double_as_longlong(dl[r]) & 0xFFFFFFFFFFFFFull;
-        const uint64_t hi = (uint64_t)__double_as_longlong(dh[r]) & 0xFFFFFFFFFFFFFull;
-        // lo + hi*2^32 as a 128-bit number (sh:sl) with lo, hi < 2^52, sh < 2^20
-        const uint64_t sl = lo + (hi << 32);
-        const uint64_t sh = (hi >> 32) + (uint64_t)(sl < lo);
-        const uint64_t v = sh * GL_EPS;  // < 2^53
-        uint64_t x = sl + v;
-        if (x < v) x += GL_EPS;
-        s[r] = x;
-    }
+    for (int r = 0; r < T5_STATE; r++) s[r] = t5_recombine(dl[r], dh[r]);
 }
 
 // x^7 on words 4..15 as two rolled groups of six (the words rotate by six per
