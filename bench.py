@@ -936,7 +936,7 @@ class ServingStream:
                 "bound_by": "gpu" if sum_gpu >= sum_copy else "host-to-device copies"}
 
 
-def serving_compact(torch, dev, h_main, h_aux, M=200, rho=1.5):
+def serving_compact(torch, dev, h_main, h_aux, M=400, rho=3.0):
     """The serving figures for the default bench line: one offered load, plain
     vs served, plus the ceiling."""
     ss = ServingStream(torch, dev, M, LOG_N, 0x7E5EED05, h_main, h_aux)

@@ -106,22 +106,21 @@ __device__ __forceinline__ uint64_t gl_reduce_limbs(uint32_t r0, uint32_t r1, ui
 }
 
 // The same reduction on the integer ALU alone (no multiply-add): x1 = r1 + r2
-// first, then r2 and r3 are subtracted from (x1:x0); the carries net to c in
-// {-1, 0, 1} (the exact value lies in [-(2^32 - 1), 2^65)), folded back as
-// above.  For kernels whose multiply-add pipe is the busier one (the Tip5
-// S-box), where the two multiply-adds of gl_reduce_limbs would queue behind the
-// product's own.
+// first, then the 33-bit sum r2 + r3 is subtracted from (x1:x0); the carries
+// net to c in {-1, 0, 1} (the exact value lies in [-(2^33 - 2), 2^65)), folded
+// back as above.  For kernels whose multiply-add pipe is the busier one (the
+// Tip5 S-box), where the two multiply-adds of gl_reduce_limbs would queue
+// behind the product's own.
 __device__ __forceinline__ uint64_t gl_reduce_limbs_alu(uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3) {
     uint32_t x0, x1;
     asm("{\n\t"
-        ".reg .u32 c, e0, e1;\n\t"
+        ".reg .u32 c, t0, t1, e0, e1;\n\t"
         "add.cc.u32 %1, %3, %4;\n\t"
         "addc.u32 c, 0, 0;\n\t"
-        "sub.cc.u32 %0, %2, %4;\n\t"
-        "subc.cc.u32 %1, %1, 0;\n\t"
-        "subc.u32 c, c, 0;\n\t"
-        "sub.cc.u32 %0, %0, %5;\n\t"
-        "subc.cc.u32 %1, %1, 0;\n\t"
+        "add.cc.u32 t0, %4, %5;\n\t"
+        "addc.u32 t1, 0, 0;\n\t"
+        "sub.cc.u32 %0, %2, t0;\n\t"
+        "subc.cc.u32 %1, %1, t1;\n\t"
         "subc.u32 c, c, 0;\n\t"
         "neg.s32 e0, c;\n\t"
         "shr.s32 e1, c, 31;\n\t"
