@@ -614,9 +614,10 @@ __global__ void __launch_bounds__(128, MINB) k_lde_mid_sym(const uint64_t* Y, ui
 // shared memory (twq, T*n1 words) and every coset reads them there; the coset
 // scale N^-1 s_c^i, i = i0 + n2*R*k1 with i0 = k2 + n2*ln, is split into a
 // per-thread factor A_c = N^-1 s_c^i0 (one per coset) and a per-CTA table
-// sb[c][k1] = s_c^(n2*R*k1); the sub-transform twiddles come from the global
-// w_4096 table through L1.  Per element and coset this replaces four global
-// table loads and one general product by two shared-memory loads.
+// sb[c][k1] = s_c^(n2*R*k1); the sub-transform twiddles stay in shared memory
+// as in k_lde_mid_sym.  Per element and coset this replaces four global table
+// loads and one general product by two shared-memory loads.  At n1 = 2^10 the
+// CTA holds 74 KB of shared memory, so three CTAs still fit on an SM.
 template <int L1, int MINB, bool RAND>
 __global__ void __launch_bounds__(128, MINB) k_lde_mid_sym2(const uint64_t* Y, uint64_t yld, uint64_t* Z, int l2,
                                                             int le, const uint64_t* tw12_f, const uint64_t* wlo,
@@ -629,9 +630,11 @@ __global__ void __launch_bounds__(128, MINB) k_lde_mid_sym2(const uint64_t* Y, u
     constexpr int lT = 7 - B, T = 1 << lT;  // T * R = 128 threads
     constexpr int n1 = 1 << L1;
     extern __shared__ uint64_t sm[];
-    uint64_t* s = sm;                          // transposes
+    uint64_t* twf = sm;                        // w_n1^m, m < n1 (forward root only)
+    uint64_t* s = twf + n1;                    // transposes
     uint64_t* twq = s + spad_words(n1, lT);    // w_N^((k20 + tt) * q) at [tt + T*q]
     uint64_t* sb = twq + (T << L1);            // s_c^(n2*R*k1) at [c*R + k1]
+    load_tw<L1>(twf, tw12_f);
     const int E = 1 << le;
     const uint64_t col = blockIdx.y;
     const uint32_t k20 = blockIdx.x << lT;
@@ -679,7 +682,7 @@ __global__ void __launch_bounds__(128, MINB) k_lde_mid_sym2(const uint64_t* Y, u
 #pragma unroll
                 for (int k = 0; k < R; k++) {
                     uint64_t x = v[brevc<B>(k)];
-                    if (ln * k) x = gl_mul_c(x, __ldg(tw12_f + ((ln * k) << (12 - L1))));
+                    if (ln * k) x = gl_mul_c(x, twf[ln * k]);
                     s[spos(ln + (k << B), lT) + t] = x;
                 }
             } else if (pass == 0) {
@@ -951,8 +954,8 @@ cudaError_t launch_lde(const LdePlan& pl, const uint64_t* trace, uint64_t tld, u
             if constexpr (Plan<L1>::NR == 2 && Plan<L1>::b1 == Plan<L1>::b2) {
                 constexpr int lTr = 7 - Plan<L1>::b2;
                 if (tuning_lde_mid_variant() == 2) {
-                    const size_t sm2 = words_bytes(spad_words(1 << L1, lTr) + ((size_t)1 << (lTr + L1)) +
-                                                   ((size_t)1 << (le + Plan<L1>::b2)));
+                    const size_t sm2 = words_bytes(((size_t)1 << L1) + spad_words(1 << L1, lTr) +
+                                                   ((size_t)1 << (lTr + L1)) + ((size_t)1 << (le + Plan<L1>::b2)));
                     auto kern = rm ? k_lde_mid_sym2<L1, 2, true>
                                    : (tuning_lde_mid_ctas() == 3 ? k_lde_mid_sym2<L1, 3, false>
                                                                  : k_lde_mid_sym2<L1, 2, false>);
