@@ -362,15 +362,16 @@ __global__ void __launch_bounds__(NTT_THREADS, L2 == 10 ? 2 : 1) k_lde_inv_a(con
     const uint64_t* src = trace + (uint64_t)blockIdx.y * tld + i10;
     uint64_t* dst = Y + (uint64_t)blockIdx.y * yld + i10;
     constexpr int n2m = (1 << L2) - 1;
+    // offsets within a column are below N <= 2^22: 32-bit index arithmetic
     sub_dft<L2, true>(
-        s, lT, tw, [&](int k, int t) { return gl_canon(src[t + ((uint64_t)(-k & n2m) << l1)]); },
+        s, lT, tw, [&](int k, int t) { return gl_canon(src[(uint32_t)t + ((uint32_t)(-k & n2m) << l1)]); },
         [](int, int, uint64_t) {});
     __syncthreads();
     const int T = 1 << lT;
     for (int idx = threadIdx.x; idx < (T << L2); idx += blockDim.x) {
         const int t = idx & (T - 1), k2 = idx >> lT;
         const uint64_t v = s[spos(out_pos<L2>(k2), lT) + t];
-        dst[t + ((uint64_t)k2 << l1)] = gl_mul_c(v, tw2(wlo, whi, (i10 + t) * (uint32_t)k2));
+        dst[(uint32_t)t + ((uint32_t)k2 << l1)] = gl_mul_c(v, tw2(wlo, whi, (i10 + t) * (uint32_t)k2));
     }
 }
 
@@ -695,11 +696,17 @@ __global__ void __launch_bounds__(128, MINB) k_lde_mid_sym2(const uint64_t* Y, u
             __syncthreads();
         }
         if (pass) {
-            uint64_t* dst = Z + (col * E + c) * N + k20;
-            for (int idx = threadIdx.x; idx < (T << L1); idx += blockDim.x) {
-                const int tt = idx & (T - 1), q = idx >> lT;
-                const uint64_t x = s[spos((q >> B) + ((q & (R - 1)) << B), lT) + tt];
-                dst[tt + ((uint64_t)q << l2)] = gl_mul_c(x, twq[idx]);
+            // thread (tt, q0) of the 128 = T x R stores X[q], q = q0 + R*m: its slot
+            // is m + R*q0, its twiddle twq[threadIdx.x + 128*m], its address
+            // dst + tt + (q0 << l2) + m*(R << l2) (bases hoisted out of the loop)
+            const int tt = threadIdx.x & (T - 1), q0 = threadIdx.x >> lT;
+            uint64_t* dst = Z + (col * E + c) * N + k20 + tt + ((uint64_t)q0 << l2);
+            const uint64_t dstep = (uint64_t)R << l2;
+            const uint64_t* twp = twq + threadIdx.x;
+#pragma unroll 4
+            for (int m = 0; m < R; m++) {
+                const uint64_t x = s[spos(m + (q0 << B), lT) + tt];
+                dst[m * dstep] = gl_mul_c(x, twp[m << 7]);
             }
             __syncthreads();
         }
@@ -726,11 +733,12 @@ __global__ void __launch_bounds__(NTT_THREADS) k_lde_fwd_b(const uint64_t* Z, ui
     uint64_t* dst = out + col * old + (uint64_t)q20 * E;
     sub_dft<L2>(
         s, lS, tw,
+        // offsets within a column are below E * N <= 2^26: 32-bit index arithmetic
         [&](int k, int u) {
-            const int c = u & (E - 1), t = u >> le;
-            return src[(uint64_t)c * N + ((uint64_t)t << L2) + k];
+            const uint32_t c = (uint32_t)u & (E - 1), t = (uint32_t)u >> le;
+            return src[(c << (l1 + L2)) + (t << L2) + (uint32_t)k];
         },
-        [&](int q, int u, uint64_t v) { dst[(((uint64_t)q << l1) * E) + u] = v; });
+        [&](int q, int u, uint64_t v) { dst[((uint32_t)q << (l1 + le)) + (uint32_t)u] = v; });
 }
 
 // N = 1: the interpolant is the constant trace value; coset c of the LDE is the
