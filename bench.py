@@ -745,12 +745,28 @@ def run_batch(args):
     for _ in range(args.warmup):
         alone()
     ms_alone = _event_ms(torch, stream, alone, args.steps)
+    # the rate a GPU-filling commit reaches (the largest table of the batch
+    # alone): the batch can go no faster than its cells at that rate
+    big = max(range(len(shapes)), key=lambda i: shapes[i][0] * shapes[i][1])
+
+    def largest():
+        n, w = shapes[big]
+        tvmc.Commitment(traces[big].data_ptr(), width=w, trace_len=n, device_ptr=True, stream=stream.cuda_stream,
+                        discard_lde=True).free()
+
+    largest()
+    ms_big = _event_ms(torch, stream, largest, args.steps)
+    big_rate = EXPANSION * shapes[big][0] * shapes[big][1] / (ms_big / 1e3)
+    ideal_ms = 1e3 * cells / big_rate
     match = True
     for i, (t, (n, w)) in enumerate(zip(traces, shapes)):
         with tvmc.Commitment(t.data_ptr(), width=w, trace_len=n, device_ptr=True) as c:
             match = match and bool((c.root() == roots[i]).all())
     line = {"metric": "committed LDE cells/s", "workload": "batch", "value": cells / (ms / 1e3), "unit": "cells/s",
             "ms_per_batch": ms, "alone_ms": ms_alone, "speedup_vs_alone": ms_alone / ms,
+            "ceiling": {"largest_table_cells_per_s": big_rate, "ideal_ms_at_that_rate": ideal_ms,
+                        "ceiling_vs_alone": ms_alone / ideal_ms,
+                        "what": "the batch's cells at the rate of its largest table committed alone"},
             "roots_equal_alone": match, "steps": args.steps, "warmup": args.warmup, "n_gpus": 1,
             "config": {"tables": len(shapes), "heights": [n for n, _ in shapes], "widths": [w for _, w in shapes],
                        "expansion": EXPANSION, "cells": cells, "tuning": tuned.get("knobs", {}),

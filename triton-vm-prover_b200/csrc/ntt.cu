@@ -46,6 +46,14 @@ constexpr int NTT_THREADS = 256;
 // Shared-memory slot of element k (T = 2^lT interleaved sequences); one row of
 // padding per 32 elements keeps every round's line accesses bank-conflict free.
 __device__ __forceinline__ int spos(int k, int lT) { return (k + (k >> 5)) << lT; }
+// The slot of k = a + (b << BITS) with a < 2^BITS: for BITS = 5 the padding
+// term k >> 5 is b itself, so the slot is (a + 33 b) << lT -- an index the
+// compiler can split into a per-line base and per-element constants.
+template <int BITS>
+__device__ __forceinline__ int spos2(int a, int b, int lT) {
+    if constexpr (BITS == 5) return (a + 33 * b) << lT;
+    else return spos(a + (b << BITS), lT);
+}
 __host__ __device__ constexpr int spad_words(int n, int lT) { return (n + (n >> 5) + 1) << lT; }
 
 // Round sizes (log2) of a 2^LS transform: one round up to 2^5, two up to 2^10,
@@ -135,7 +143,7 @@ __device__ __forceinline__ void sub_dft(uint64_t* s, int lT, const uint64_t* tw,
             for (int k2 = 0; k2 < R2; k2++) {
                 uint64_t x = v[brevc<b2>(k2)];
                 if (k2) x = gl_mul_c(x, tw[d1 * k2]);
-                s[spos(d1 + (k2 << b1), lT) + t] = x;
+                s[spos2<b1>(d1, k2, lT) + t] = x;
             }
         }
         __syncthreads();
@@ -144,11 +152,11 @@ __device__ __forceinline__ void sub_dft(uint64_t* s, int lT, const uint64_t* tw,
             const int t = id & (T - 1), k2 = id >> lT;
             uint64_t v[R1];
 #pragma unroll
-            for (int d1 = 0; d1 < R1; d1++) v[d1] = s[spos(d1 + (k2 << b1), lT) + t];
+            for (int d1 = 0; d1 < R1; d1++) v[d1] = s[spos2<b1>(d1, k2, lT) + t];
             reg_dft<b1>(v);
 #pragma unroll
             for (int k1 = 0; k1 < R1; k1++) {
-                if constexpr (TO_SMEM) s[spos(k1 + (k2 << b1), lT) + t] = v[brevc<b1>(k1)];
+                if constexpr (TO_SMEM) s[spos2<b1>(k1, k2, lT) + t] = v[brevc<b1>(k1)];
                 else store((k1 << b2) + k2, t, v[brevc<b1>(k1)]);
             }
         }
@@ -463,7 +471,7 @@ __global__ void __launch_bounds__(128) k_lde_mid_reg(const uint64_t* Y, uint64_t
         for (int k2 = 0; k2 < R2; k2++) {
             uint64_t x = v[brevc<b2>(k2)];
             if (k2) x = gl_mul_c(x, twf[d1 * k2]);
-            s[spos(d1 + (k2 << b1), lT) + t] = x;
+            s[spos2<b1>(d1, k2, lT) + t] = x;
         }
     }
     __syncthreads();
@@ -579,7 +587,7 @@ __global__ void __launch_bounds__(128, MINB) k_lde_mid_sym(const uint64_t* Y, ui
                 }
             } else {  // round 2 of either: slots x + R*ln
 #pragma unroll
-                for (int x = 0; x < R; x++) v[x] = s[spos(x + (ln << B), lT) + t];
+                for (int x = 0; x < R; x++) v[x] = s[spos2<B>(x, ln, lT) + t];
             }
             reg_dft<B>(v);
             if (half == 0) {  // twiddle w^(ln*k), slot ln + R*k
@@ -587,14 +595,14 @@ __global__ void __launch_bounds__(128, MINB) k_lde_mid_sym(const uint64_t* Y, ui
                 for (int k = 0; k < R; k++) {
                     uint64_t x = v[brevc<B>(k)];
                     if (ln * k) x = gl_mul_c(x, tw[ln * k]);
-                    s[spos(ln + (k << B), lT) + t] = x;
+                    s[spos2<B>(ln, k, lT) + t] = x;
                 }
             } else if (pass == 0) {
 #pragma unroll
                 for (int k1 = 0; k1 < R; k1++) cf[k1] = v[brevc<B>(k1)];
             } else {  // X[R*q1 + ln] stays in slot q1 + R*ln
 #pragma unroll
-                for (int q1 = 0; q1 < R; q1++) s[spos(q1 + (ln << B), lT) + t] = v[brevc<B>(q1)];
+                for (int q1 = 0; q1 < R; q1++) s[spos2<B>(q1, ln, lT) + t] = v[brevc<B>(q1)];
             }
             __syncthreads();
         }
@@ -676,7 +684,7 @@ __global__ void __launch_bounds__(128, MINB) k_lde_mid_sym2(const uint64_t* Y, u
                 }
             } else {  // round 2 of either: slots x + R*ln
 #pragma unroll
-                for (int x = 0; x < R; x++) v[x] = s[spos(x + (ln << B), lT) + t];
+                for (int x = 0; x < R; x++) v[x] = s[spos2<B>(x, ln, lT) + t];
             }
             reg_dft<B>(v);
             if (half == 0) {  // twiddle w_n1^(ln*k), slot ln + R*k
@@ -684,14 +692,14 @@ __global__ void __launch_bounds__(128, MINB) k_lde_mid_sym2(const uint64_t* Y, u
                 for (int k = 0; k < R; k++) {
                     uint64_t x = v[brevc<B>(k)];
                     if (ln * k) x = gl_mul_c(x, twf[ln * k]);
-                    s[spos(ln + (k << B), lT) + t] = x;
+                    s[spos2<B>(ln, k, lT) + t] = x;
                 }
             } else if (pass == 0) {
 #pragma unroll
                 for (int k1 = 0; k1 < R; k1++) cf[k1] = v[brevc<B>(k1)];
             } else {  // X[R*q1 + ln] stays in slot q1 + R*ln
 #pragma unroll
-                for (int q1 = 0; q1 < R; q1++) s[spos(q1 + (ln << B), lT) + t] = v[brevc<B>(q1)];
+                for (int q1 = 0; q1 < R; q1++) s[spos2<B>(q1, ln, lT) + t] = v[brevc<B>(q1)];
             }
             __syncthreads();
         }
@@ -705,7 +713,7 @@ __global__ void __launch_bounds__(128, MINB) k_lde_mid_sym2(const uint64_t* Y, u
             const uint64_t* twp = twq + threadIdx.x;
 #pragma unroll 4
             for (int m = 0; m < R; m++) {
-                const uint64_t x = s[spos(m + (q0 << B), lT) + tt];
+                const uint64_t x = s[spos2<B>(m, q0, lT) + tt];
                 dst[m * dstep] = gl_mul_c(x, twp[m << 7]);
             }
             __syncthreads();
