@@ -418,6 +418,10 @@ def run_reference_gpu(args):
         d["lde"].append(ev[0].elapsed_time(ev[1]))
         d["row_hash"].append(ev[1].elapsed_time(ev[2]))
         d["merkle"].append(ev[2].elapsed_time(ev[3]))
+    # per-step spread: the reference's LDE allocates and frees scratch inside
+    # every call (cudaMalloc/cudaFree in randomized_lde_batch_impl), so its
+    # stage times vary with the host and the allocator's state
+    spread = {k: {s: [round(min(v), 2), round(max(v), 2)] for s, v in d.items()} for k, d in stages.items()}
     stages = {k: {s: statistics.median(v) for s, v in d.items()} for k, d in stages.items()}
     cells = L * (W_MAIN + W_AUX)
     line = {"metric": METRIC, "impl": "reference", "workload": "reference GPU kernels (sm_100a build)",
@@ -428,7 +432,8 @@ def run_reference_gpu(args):
                                    "(offset 7), Tip5 row hash, Merkle (two trees)", "trace_len": n, "lde_len": L,
                        "traces": "resident in HBM", "kernels": "randomized_lde_batch_gpu_preallocated (no "
                        "randomizers), hash_bfield_rows_gpu / hash_xfield_rows_gpu, merkle_tree_gpu"},
-            "stage_ms_per_table": stages, "parity_2p10x379_vs_oracle": parity, "clocks": clk.summary()}
+            "stage_ms_per_table": stages, "stage_ms_min_max": spread,
+            "parity_2p10x379_vs_oracle": parity, "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
 
 
