@@ -176,22 +176,22 @@ __device__ __forceinline__ uint64_t gl_add_pc(uint64_t a, uint64_t b) {
     return ((uint64_t)r1 << 32) | r0;
 }
 
-// Canonical add of canonical operands: s = a + b (65 bits); s - p is s + 2^32 - 1
-// modulo 2^64, taken when either addition carries.
+// Canonical add of canonical operands as a subtraction: a + b = a - (p - b),
+// where p - b lies in [1, p]; a borrow adds p back (subtracts 2^32 - 1 modulo
+// 2^64), which cannot borrow again because the wrapped difference is at least
+// 2^64 - p = 2^32 - 1.  Seven instructions against nine for the add-then-
+// compare form.
 __device__ __forceinline__ uint64_t gl_add_c(uint64_t a, uint64_t b) {
     uint32_t r0, r1;
     asm("{\n\t"
-        ".reg .u32 s0, s1, t0, t1, c;\n\t"
-        ".reg .pred q;\n\t"
-        "add.cc.u32 s0, %2, %4;\n\t"
-        "addc.cc.u32 s1, %3, %5;\n\t"
-        "addc.u32 c, 0, 0;\n\t"
-        "add.cc.u32 t0, s0, 0xFFFFFFFF;\n\t"
-        "addc.cc.u32 t1, s1, 0;\n\t"
-        "addc.u32 c, c, 0;\n\t"
-        "setp.ne.u32 q, c, 0;\n\t"
-        "selp.b32 %0, t0, s0, q;\n\t"
-        "selp.b32 %1, t1, s1, q;\n\t"
+        ".reg .u32 n0, n1, s0, s1, m;\n\t"
+        "sub.cc.u32 n0, 1, %4;\n\t"
+        "subc.u32 n1, 0xFFFFFFFF, %5;\n\t"
+        "sub.cc.u32 s0, %2, n0;\n\t"
+        "subc.cc.u32 s1, %3, n1;\n\t"
+        "subc.u32 m, 0, 0;\n\t"
+        "sub.cc.u32 %0, s0, m;\n\t"
+        "subc.u32 %1, s1, 0;\n\t"
         "}"
         : "=r"(r0), "=r"(r1)
         : "r"((uint32_t)a), "r"((uint32_t)(a >> 32)), "r"((uint32_t)b), "r"((uint32_t)(b >> 32)));
