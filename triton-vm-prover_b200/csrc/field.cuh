@@ -215,6 +215,67 @@ __device__ __forceinline__ uint64_t gl_sub_c(uint64_t a, uint64_t b) {
     return ((uint64_t)r1 << 32) | r0;
 }
 
+// ---- Montgomery products ---------------------------------------------------
+// With R = 2^64, the Montgomery reduction of a 128-bit T = (r3:r2:r1:r0) is
+// T * R^-1 (mod p) = (T - m p) / 2^64 for m = T * p^-1 (mod 2^64), and
+// p^-1 = 1 + 2^32 (mod 2^64) makes m = a = lo + (lo << 32) (mod 2^64), lo =
+// (r1:r0), with carry e; then (m p) >> 64 = a - (a >> 32) - e =: b, and the
+// result is hi - b, plus p on a borrow.  For T < p * 2^64 (one factor below p)
+// the result is canonical; for any T it is a 64-bit representative.  Nine
+// instructions: a's high limb plus its carry, t = a1 + e, cannot wrap (a carry
+// leaves a1 <= 2^32 - 2), so b = (a1 : r0) - t is one two-limb subtraction.
+__device__ __forceinline__ uint64_t gl_redc(uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3) {
+    uint32_t x0, x1;
+    asm("{\n\t"
+        ".reg .u32 a1, t, b0, b1, c;\n\t"
+        "add.cc.u32 a1, %3, %2;\n\t"
+        "addc.u32 t, a1, 0;\n\t"
+        "sub.cc.u32 b0, %2, t;\n\t"
+        "subc.u32 b1, a1, 0;\n\t"
+        "sub.cc.u32 %0, %4, b0;\n\t"
+        "subc.cc.u32 %1, %5, b1;\n\t"
+        "subc.u32 c, 0, 0;\n\t"
+        "sub.cc.u32 %0, %0, c;\n\t"
+        "subc.u32 %1, %1, 0;\n\t"
+        "}"
+        : "=r"(x0), "=r"(x1)
+        : "r"(r0), "r"(r1), "r"(r2), "r"(r3));
+    return ((uint64_t)x1 << 32) | x0;
+}
+
+// x * w for any 64-bit x and a factor given in Montgomery form wm = w * 2^64
+// (mod p), wm < p; canonical.
+__device__ __forceinline__ uint64_t gl_mont_mul(uint64_t x, uint64_t wm) {
+    uint32_t r0, r1, r2, r3;
+    gl_mul128(x, wm, r0, r1, r2, r3);
+    return gl_redc(r0, r1, r2, r3);
+}
+
+// x * 2^-64 (mod p), canonical, for any 64-bit x (the reduction of T = x < p * 2^64).
+__device__ __forceinline__ uint64_t gl_from_mont(uint64_t x) {
+    return gl_redc((uint32_t)x, (uint32_t)(x >> 32), 0u, 0u);
+}
+
+// x * 2^64 (mod p), canonical, for any 64-bit x = x1 * 2^32 + x0: 2^64 = 2^32 - 1
+// and 2^96 = -1 give x0 * (2^32 - 1) - x1, whose positive part is below p; a
+// borrow adds p (subtracts 2^32 - 1 modulo 2^64) and cannot recur.
+__device__ __forceinline__ uint64_t gl_to_mont(uint64_t x) {
+    uint32_t m0, m1;
+    asm("{\n\t"
+        ".reg .u32 t0, t1, k;\n\t"
+        "sub.cc.u32 t0, 0, %2;\n\t"
+        "subc.u32 t1, %2, 0;\n\t"
+        "sub.cc.u32 %0, t0, %3;\n\t"
+        "subc.cc.u32 %1, t1, 0;\n\t"
+        "subc.u32 k, 0, 0;\n\t"
+        "sub.cc.u32 %0, %0, k;\n\t"
+        "subc.u32 %1, %1, 0;\n\t"
+        "}"
+        : "=r"(m0), "=r"(m1)
+        : "r"((uint32_t)x), "r"((uint32_t)(x >> 32)));
+    return ((uint64_t)m1 << 32) | m0;
+}
+
 // ---- multiplication by powers of two -------------------------------------
 // 2 has order 192 mod p (2^96 = -1), so every root of unity of order <= 64 is
 // +-2^s with s < 96: a shift and a short reduction instead of a multiply.  The

@@ -102,6 +102,14 @@ __device__ __forceinline__ void reg_dft(uint64_t (&v)[1 << B]) {
     }
 }
 
+// x times a twiddle from a table: plain (canonical product) or, with MONT, a
+// table in Montgomery form (gl_mont_mul: seven fewer instructions).
+template <bool MONT>
+__device__ __forceinline__ uint64_t tw_mul(uint64_t x, uint64_t w) {
+    if constexpr (MONT) return gl_mont_mul(x, w);
+    else return gl_mul_c(x, w);
+}
+
 // DFT of size 2^LS on T = 2^lT sequences.  load(k, t) returns input element k
 // of sequence t (called once per element, by the first round); store(k, t, v)
 // receives output X[k] of sequence t (called once, by the last round).  With
@@ -113,7 +121,7 @@ __device__ __forceinline__ void reg_dft(uint64_t (&v)[1 << B]) {
 // anything a store wrote to shared memory.  The transform is the forward one
 // (tw holds powers of the forward root; callers negate input indices for an
 // inverse).
-template <int LS, bool TO_SMEM = false, class LoadF, class StoreF>
+template <int LS, bool TO_SMEM = false, bool MONT = false, class LoadF, class StoreF>
 __device__ __forceinline__ void sub_dft(uint64_t* s, int lT, const uint64_t* tw, LoadF&& load, StoreF&& store) {
     using PL = Plan<LS>;
     const int T = 1 << lT;
@@ -142,7 +150,7 @@ __device__ __forceinline__ void sub_dft(uint64_t* s, int lT, const uint64_t* tw,
 #pragma unroll
             for (int k2 = 0; k2 < R2; k2++) {
                 uint64_t x = v[brevc<b2>(k2)];
-                if (k2) x = gl_mul_c(x, tw[d1 * k2]);
+                if (k2) x = tw_mul<MONT>(x, tw[d1 * k2]);
                 s[spos2<b1>(d1, k2, lT) + t] = x;
             }
         }
@@ -174,7 +182,7 @@ __device__ __forceinline__ void sub_dft(uint64_t* s, int lT, const uint64_t* tw,
             for (int k3 = 0; k3 < R3; k3++) {
                 uint64_t x = v[brevc<b3>(k3)];
                 const int e = ((lo >> b1) * k3) << b1;
-                if (e) x = gl_mul_c(x, tw[e]);
+                if (e) x = tw_mul<MONT>(x, tw[e]);
                 s[spos(lo + (k3 << (b1 + b2)), lT) + t] = x;
             }
         }
@@ -192,7 +200,7 @@ __device__ __forceinline__ void sub_dft(uint64_t* s, int lT, const uint64_t* tw,
             for (int k2 = 0; k2 < R2; k2++) {
                 uint64_t x = v[brevc<b2>(k2)];
                 const int e = d1 * (R3 * k2 + k3);
-                if (e) x = gl_mul_c(x, tw[e]);
+                if (e) x = tw_mul<MONT>(x, tw[e]);
                 s[spos(base + (k2 << b1), lT) + t] = x;
             }
         }
@@ -235,10 +243,14 @@ __device__ __forceinline__ uint64_t tw2(const uint64_t* __restrict__ lo, const u
     return gl_mul(__ldg(lo + (e & 4095)), __ldg(hi + (e >> 12)));
 }
 
-// tw[e] = w_{2^LS}^e, e < 2^LS, from the 4096-entry table of w_4096 powers.
-template <int LS>
+// tw[e] = w_{2^LS}^e, e < 2^LS, from the 4096-entry table of w_4096 powers
+// (with MONT in Montgomery form, w * 2^64).
+template <int LS, bool MONT = false>
 __device__ __forceinline__ void load_tw(uint64_t* tw, const uint64_t* __restrict__ tw12) {
-    for (int m = threadIdx.x; m < (1 << LS); m += blockDim.x) tw[m] = __ldg(tw12 + (m << (12 - LS)));
+    for (int m = threadIdx.x; m < (1 << LS); m += blockDim.x) {
+        const uint64_t w = __ldg(tw12 + (m << (12 - LS)));
+        tw[m] = MONT ? gl_to_mont(w) : w;
+    }
 }
 
 // ---------------------------------------------------------------- plain NTT
@@ -364,14 +376,14 @@ __global__ void __launch_bounds__(NTT_THREADS, L2 == 10 ? 2 : 1) k_lde_inv_a(con
     extern __shared__ uint64_t sm[];
     uint64_t* tw = sm;
     uint64_t* s = sm + (1 << L2);
-    load_tw<L2>(tw, tw12_f);
+    load_tw<L2, true>(tw, tw12_f);
     __syncthreads();
     const uint32_t i10 = blockIdx.x << lT;
     const uint64_t* src = trace + (uint64_t)blockIdx.y * tld + i10;
     uint64_t* dst = Y + (uint64_t)blockIdx.y * yld + i10;
     constexpr int n2m = (1 << L2) - 1;
     // offsets within a column are below N <= 2^22: 32-bit index arithmetic
-    sub_dft<L2, true>(
+    sub_dft<L2, true, true>(
         s, lT, tw, [&](int k, int t) { return gl_canon(src[(uint32_t)t + ((uint32_t)(-k & n2m) << l1)]); },
         [](int, int, uint64_t) {});
     __syncthreads();
@@ -643,17 +655,17 @@ __global__ void __launch_bounds__(128, MINB) k_lde_mid_sym2(const uint64_t* Y, u
     uint64_t* s = twf + n1;                    // transposes
     uint64_t* twq = s + spad_words(n1, lT);    // w_N^((k20 + tt) * q) at [tt + T*q]
     uint64_t* sb = twq + (T << L1);            // s_c^(n2*R*k1) at [c*R + k1]
-    load_tw<L1>(twf, tw12_f);
+    load_tw<L1, true>(twf, tw12_f);
     const int E = 1 << le;
     const uint64_t col = blockIdx.y;
     const uint32_t k20 = blockIdx.x << lT;
     const uint64_t N = 1ull << (L1 + l2);
     for (int idx = threadIdx.x; idx < (T << L1); idx += blockDim.x)
-        twq[idx] = tw2(wlo, whi, (k20 + (idx & (T - 1))) * (uint32_t)(idx >> lT));
+        twq[idx] = gl_to_mont(tw2(wlo, whi, (k20 + (idx & (T - 1))) * (uint32_t)(idx >> lT)));
     for (int idx = threadIdx.x; idx < (E << B); idx += blockDim.x) {
         const int c = idx >> B, k1 = idx & (R - 1);
         // tw2 on the scale tables carries N^-1; multiplying by N cancels it
-        sb[idx] = gl_mul_c(tw2(sc_lo + 4096 * c, sc_hi + hi_len * c, ((uint32_t)k1 << (B + l2))), N);
+        sb[idx] = gl_to_mont(gl_mul(tw2(sc_lo + 4096 * c, sc_hi + hi_len * c, ((uint32_t)k1 << (B + l2))), N));
     }
     __syncthreads();
     const uint64_t* src = Y + col * yld + ((uint64_t)k20 << L1);
@@ -663,7 +675,7 @@ __global__ void __launch_bounds__(128, MINB) k_lde_mid_sym2(const uint64_t* Y, u
 #pragma unroll 1
     for (int pass = 0; pass <= E; pass++) {  // 0: inverse; c + 1: forward, coset c
         const int c = pass ? pass - 1 : 0;
-        const uint64_t a_c = tw2(sc_lo + 4096 * c, sc_hi + hi_len * c, i0);
+        const uint64_t a_c = gl_to_mont(tw2(sc_lo + 4096 * c, sc_hi + hi_len * c, i0));
 #pragma unroll 1
         for (int half = 0; half < 2; half++) {
             uint64_t v[R];
@@ -679,7 +691,7 @@ __global__ void __launch_bounds__(128, MINB) k_lde_mid_sym2(const uint64_t* Y, u
                             const uint32_t i = i0 + ((uint32_t)k1 << (B + l2));
                             if (i < (uint32_t)rm) x = gl_add_pc(x, add[(col * E + c) * rm + i]);
                         }
-                        v[k1] = gl_mul_c(gl_mul(x, sb[c * R + k1]), a_c);
+                        v[k1] = gl_mont_mul(gl_mont_mul(x, sb[c * R + k1]), a_c);
                     }
                 }
             } else {  // round 2 of either: slots x + R*ln
@@ -691,7 +703,7 @@ __global__ void __launch_bounds__(128, MINB) k_lde_mid_sym2(const uint64_t* Y, u
 #pragma unroll
                 for (int k = 0; k < R; k++) {
                     uint64_t x = v[brevc<B>(k)];
-                    if (ln * k) x = gl_mul_c(x, twf[ln * k]);
+                    if (ln * k) x = gl_mont_mul(x, twf[ln * k]);
                     s[spos2<B>(ln, k, lT) + t] = x;
                 }
             } else if (pass == 0) {
@@ -714,7 +726,7 @@ __global__ void __launch_bounds__(128, MINB) k_lde_mid_sym2(const uint64_t* Y, u
 #pragma unroll 4
             for (int m = 0; m < R; m++) {
                 const uint64_t x = s[spos2<B>(m, q0, lT) + tt];
-                dst[m * dstep] = gl_mul_c(x, twp[m << 7]);
+                dst[m * dstep] = gl_mont_mul(x, twp[m << 7]);
             }
             __syncthreads();
         }
@@ -732,14 +744,14 @@ __global__ void __launch_bounds__(NTT_THREADS) k_lde_fwd_b(const uint64_t* Z, ui
     const int lS = lT3 + le;
     uint64_t* tw = sm;
     uint64_t* s = sm + (1 << L2);
-    load_tw<L2>(tw, tw12_f);
+    load_tw<L2, true>(tw, tw12_f);
     __syncthreads();
     const uint64_t col = blockIdx.y;
     const uint32_t q20 = blockIdx.x << lT3;
     const uint64_t N = 1ull << (l1 + L2);
     const uint64_t* src = Z + col * E * N + ((uint64_t)q20 << L2);
     uint64_t* dst = out + col * old + (uint64_t)q20 * E;
-    sub_dft<L2>(
+    sub_dft<L2, false, true>(
         s, lS, tw,
         // offsets within a column are below E * N <= 2^26: 32-bit index arithmetic
         [&](int k, int u) {
