@@ -105,33 +105,6 @@ __device__ __forceinline__ uint64_t gl_reduce_limbs(uint32_t r0, uint32_t r1, ui
     return ((uint64_t)x1 << 32) | x0;
 }
 
-// The same reduction on the integer ALU alone (no multiply-add): x1 = r1 + r2
-// first, then the 33-bit sum r2 + r3 is subtracted from (x1:x0); the carries
-// net to c in {-1, 0, 1} (the exact value lies in [-(2^33 - 2), 2^65)), folded
-// back as above.  For kernels whose multiply-add pipe is the busier one (the
-// Tip5 S-box), where the two multiply-adds of gl_reduce_limbs would queue
-// behind the product's own.
-__device__ __forceinline__ uint64_t gl_reduce_limbs_alu(uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3) {
-    uint32_t x0, x1;
-    asm("{\n\t"
-        ".reg .u32 c, t0, t1, e0, e1;\n\t"
-        "add.cc.u32 %1, %3, %4;\n\t"
-        "addc.u32 c, 0, 0;\n\t"
-        "add.cc.u32 t0, %4, %5;\n\t"
-        "addc.u32 t1, 0, 0;\n\t"
-        "sub.cc.u32 %0, %2, t0;\n\t"
-        "subc.cc.u32 %1, %1, t1;\n\t"
-        "subc.u32 c, c, 0;\n\t"
-        "neg.s32 e0, c;\n\t"
-        "shr.s32 e1, c, 31;\n\t"
-        "add.cc.u32 %0, %0, e0;\n\t"
-        "addc.u32 %1, %1, e1;\n\t"
-        "}"
-        : "=r"(x0), "=r"(x1)
-        : "r"(r0), "r"(r1), "r"(r2), "r"(r3));
-    return ((uint64_t)x1 << 32) | x0;
-}
-
 // a * b for any 64-bit representatives; partial result.
 __device__ __forceinline__ uint64_t gl_mul(uint64_t a, uint64_t b) {
     uint32_t r0, r1, r2, r3;
@@ -142,20 +115,6 @@ __device__ __forceinline__ uint64_t gl_mul(uint64_t a, uint64_t b) {
 __device__ __forceinline__ uint64_t gl_mul_c(uint64_t a, uint64_t b) { return gl_canon(gl_mul(a, b)); }
 
 __device__ __forceinline__ uint64_t gl_sqr(uint64_t a) { return gl_mul(a, a); }
-
-// a^2 through gl_sqr128, reduced on the ALU; partial result.
-__device__ __forceinline__ uint64_t gl_sqr_alu(uint64_t a) {
-    uint32_t r0, r1, r2, r3;
-    gl_sqr128(a, r0, r1, r2, r3);
-    return gl_reduce_limbs_alu(r0, r1, r2, r3);
-}
-
-// a * b with the reduction on the ALU (gl_reduce_limbs_alu); partial result.
-__device__ __forceinline__ uint64_t gl_mul_alu(uint64_t a, uint64_t b) {
-    uint32_t r0, r1, r2, r3;
-    gl_mul128(a, b, r0, r1, r2, r3);
-    return gl_reduce_limbs_alu(r0, r1, r2, r3);
-}
 
 // a + b where b < p (a any representative); partial result.  A carry out of
 // 64 bits means the sum exceeds 2^64 by less than p, so adding 2^32 - 1 (i.e.

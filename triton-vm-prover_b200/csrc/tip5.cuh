@@ -2,24 +2,27 @@
 //
 // Semantics follow the reference's Tip5 (src/hash/tip5.cpp:92-203): 16-word
 // state, 5 rounds of [S-box -> MDS -> round constants].  The S-box applies
-// split-and-lookup to words 0-3 (to Montgomery form, byte-wise table, back)
-// and x^7 to words 4-15; the MDS is the circulant matrix whose first column is
-// given below.  The byte table is the offset Fermat cube map x -> (x+1)^3 - 1
-// over F_257, generated here rather than tabulated.
+// split-and-lookup to words 0-3 (a byte-wise table on the Montgomery
+// representation) and x^7 to words 4-15; the MDS is the circulant matrix whose
+// first column is given below.  The byte table is the offset Fermat cube map
+// x -> (x+1)^3 - 1 over F_257, generated here rather than tabulated.
 //
 // B200 layout choices (measured on sm_100a: 32-bit IMAD and DFMA are
 // half-rate, IMAD.HI quarter-rate, IMAD.WIDE takes two issue slots):
+//   * the hashing kernels keep the state in Montgomery form (w * 2^64 mod p,
+//     the representation the reference's BFieldElement holds), converting at
+//     absorb and squeeze only: the byte lookups then need no conversion, and
+//     every x^7 product reduces by a nine-instruction Montgomery reduction
+//     (gl_redc) instead of a two-step reduction and canonicalisation;
 //   * the byte table lives in shared memory as 256 words x 32 lanes, one
 //     entry per word and every lane owning its own bank, so the 8 lookups per
 //     word never conflict and the looked-up bytes are assembled by byte
 //     permutes with constant selectors;
 //   * the MDS runs exactly on the FP64 pipe (t5_mds), in parallel with the
-//     integer S-box work on the ALU/FMA pipes;
-//   * x^7 is a rolled loop over two groups of six words; three of its four
-//     products are reduced on the ALU (gl_sqr_alu, gl_mul_alu) and the squares
-//     take three partial products, which balances the ALU and multiply-add
-//     pipes (the 32-bit multiply-adds of the products alone would keep the
-//     multiply-add pipe the busier one).
+//     integer S-box work on the ALU/FMA pipes; being linear with integer
+//     entries it commutes with the Montgomery form, and its round constants
+//     are stored in that form;
+//   * x^7 is a rolled loop over two groups of six words (instruction cache).
 #pragma once
 #include <cstdint>
 #include "field.cuh"
@@ -43,19 +46,28 @@ constexpr double t5_mds_column_sum() {
 // 2^52 + 2^31 * sum(M): the output bias of a centred half-product (t5_mds_half).
 constexpr double T5_MDS_BIAS = 4503599627370496.0 + 2147483648.0 * t5_mds_column_sum();
 
+// x * 2^64 (mod p) at compile time: x0 * (2^32 - 1) - x1 for x = x1 * 2^32 + x0.
+constexpr uint64_t t5_to_mont_const(uint64_t x) {
+    const uint64_t v = (x & 0xFFFFFFFFull) * 0xFFFFFFFFull, x1 = x >> 32;
+    return v >= x1 ? v - x1 : GL_P - (x1 - v);
+}
+// The round constants enter in Montgomery form, like the state (t5_permutation_m).
 struct T5RoundBias {
-    double lo[T5_ROUNDS * T5_STATE];  // T5_MDS_BIAS + (rc & (2^32 - 1))
-    double hi[T5_ROUNDS * T5_STATE];  // T5_MDS_BIAS + (rc >> 32)
+    double lo[T5_ROUNDS * T5_STATE];  // T5_MDS_BIAS + (rc * 2^64 mod p) & (2^32 - 1)
+    double hi[T5_ROUNDS * T5_STATE];  // T5_MDS_BIAS + (rc * 2^64 mod p) >> 32
 };
 constexpr T5RoundBias t5_round_bias() {
     const uint64_t rc[T5_ROUNDS * T5_STATE] = {TVMC_T5_ROUND_CONSTANTS};
     T5RoundBias b{};
     for (int i = 0; i < T5_ROUNDS * T5_STATE; i++) {
-        b.lo[i] = T5_MDS_BIAS + (double)(uint32_t)rc[i];
-        b.hi[i] = T5_MDS_BIAS + (double)(uint32_t)(rc[i] >> 32);
+        const uint64_t m = t5_to_mont_const(rc[i]);
+        b.lo[i] = T5_MDS_BIAS + (double)(uint32_t)m;
+        b.hi[i] = T5_MDS_BIAS + (double)(uint32_t)(m >> 32);
     }
     return b;
 }
+// 1 in Montgomery form (2^64 mod p): the capacity of hash_pair and the padding 1.
+constexpr uint64_t T5_MONT_ONE = 0xFFFFFFFFull;
 __device__ __constant__ T5RoundBias c_t5_bias = t5_round_bias();
 
 // Shared-memory S-box table (32 KB): word v*32 + l holds the table byte for
@@ -93,53 +105,29 @@ __device__ __forceinline__ uint32_t t5_lookup32(uint32_t m, const uint32_t* lane
     return __byte_perm(__byte_perm(w0, w1, 0x0040), __byte_perm(w2, w3, 0x0040), 0x5410);
 }
 
-// split_and_lookup (src/hash/tip5.cpp:119-145) for any representative x; the
-// result is a representative in [1, p] (p for zero), which the MDS accepts.
-// Both Montgomery conversions are 32-bit carry chains:
-//   in:  x * 2^64 = x0*(2^32 - 1) - x1 (mod p) for x = x1*2^32 + x0: the
-//        difference (x0*2^32 - x0) - x1 is canonical, or wraps once and is
-//        corrected by adding p (subtracting 2^32 - 1 modulo 2^64);
-//   out: y * 2^-64 = p - b with b = a - (a >> 32) - [a < y] (mod 2^64) and
-//        a = y + (y << 32) (mod 2^64), the reduction of y by the Montgomery
-//        factor p^-1 = 2^32 + 1 (mod 2^64).
-__device__ __forceinline__ uint64_t t5_split_lookup(uint64_t x, const uint32_t* lane_tbl) {
-    uint32_t m0, m1;
-    asm("{\n\t"
-        ".reg .u32 t0, t1, k;\n\t"
-        "sub.cc.u32 t0, 0, %2;\n\t"
-        "subc.u32 t1, %2, 0;\n\t"
-        "sub.cc.u32 %0, t0, %3;\n\t"
-        "subc.cc.u32 %1, t1, 0;\n\t"
-        "subc.u32 k, 0, 0;\n\t"
-        "sub.cc.u32 %0, %0, k;\n\t"
-        "subc.u32 %1, %1, 0;\n\t"
-        "}"
-        : "=r"(m0), "=r"(m1)
-        : "r"((uint32_t)x), "r"((uint32_t)(x >> 32)));
-    const uint32_t y0 = t5_lookup32(m0, lane_tbl);
-    const uint32_t y1 = t5_lookup32(m1, lane_tbl);
-    uint32_t r0, r1;
-    asm("{\n\t"
-        ".reg .u32 a1, c, b0, b1;\n\t"
-        "add.cc.u32 a1, %3, %2;\n\t"
-        "addc.u32 c, 0, 0;\n\t"
-        "sub.cc.u32 b0, %2, a1;\n\t"
-        "subc.u32 b1, a1, 0;\n\t"
-        "sub.cc.u32 b0, b0, c;\n\t"
-        "subc.u32 b1, b1, 0;\n\t"
-        "sub.cc.u32 %0, 1, b0;\n\t"
-        "subc.u32 %1, 0xFFFFFFFF, b1;\n\t"
-        "}"
-        : "=r"(r0), "=r"(r1)
-        : "r"(y0), "r"(y1));
-    return ((uint64_t)r1 << 32) | r0;
+// split_and_lookup on a state word held in Montgomery form (t5_permutation_m):
+// the reference applies the byte table to the canonical Montgomery
+// representation and keeps the result as the new Montgomery representation
+// (src/hash/tip5.cpp:119-145), so only a canonicalisation precedes the lookups.
+__device__ __forceinline__ uint64_t t5_split_lookup_m(uint64_t x, const uint32_t* lane_tbl) {
+    const uint64_t y = gl_canon(x);
+    const uint32_t y0 = t5_lookup32((uint32_t)y, lane_tbl);
+    const uint32_t y1 = t5_lookup32((uint32_t)(y >> 32), lane_tbl);
+    return ((uint64_t)y1 << 32) | y0;
 }
 
-__device__ __forceinline__ uint64_t t5_pow7(uint64_t x) {
-    uint64_t x2 = gl_sqr_alu(x);
-    uint64_t x3 = gl_mul_alu(x, x2);
-    uint64_t x4 = gl_sqr_alu(x2);
-    return gl_mul(x3, x4);  // reduced on the multiply-add pipe: the two pipes balance
+// x^7 of a Montgomery-form word: four Montgomery products (gl_redc, nine ALU
+// instructions each); any 64-bit representative in and out.
+__device__ __forceinline__ uint64_t t5_pow7_m(uint64_t x) {
+    uint32_t r0, r1, r2, r3;
+    gl_sqr128(x, r0, r1, r2, r3);
+    const uint64_t x2 = gl_redc(r0, r1, r2, r3);
+    gl_mul128(x, x2, r0, r1, r2, r3);
+    const uint64_t x3 = gl_redc(r0, r1, r2, r3);
+    gl_sqr128(x2, r0, r1, r2, r3);
+    const uint64_t x4 = gl_redc(r0, r1, r2, r3);
+    gl_mul128(x3, x4, r0, r1, r2, r3);
+    return gl_redc(r0, r1, r2, r3);
 }
 
 // Circulant MDS: out[r] = sum_c M[(r - c) mod 16] * s[c] (mod p), i.e. the
@@ -268,11 +256,11 @@ __device__ __forceinline__ void t5_mds(uint64_t s[T5_STATE], int rnd) {
 // group), which keeps the round body small enough for the instruction cache;
 // two groups of six measured 1% faster than three of four (fewer register
 // moves), twelve unrolled 3% slower.
-__device__ __forceinline__ void t5_pow7_layer(uint64_t s[T5_STATE]) {
+__device__ __forceinline__ void t5_pow7_layer_m(uint64_t s[T5_STATE]) {
 #pragma unroll 1
     for (int g = 0; g < 2; g++) {
 #pragma unroll
-        for (int i = 4; i < 10; i++) s[i] = t5_pow7(s[i]);
+        for (int i = 4; i < 10; i++) s[i] = t5_pow7_m(s[i]);
         uint64_t t[6];
 #pragma unroll
         for (int i = 0; i < 6; i++) t[i] = s[4 + i];
@@ -283,36 +271,55 @@ __device__ __forceinline__ void t5_pow7_layer(uint64_t s[T5_STATE]) {
     }
 }
 
-__device__ __forceinline__ void t5_permutation(uint64_t s[T5_STATE], const uint32_t* lane_tbl) {
+// The permutation on a state held in Montgomery form (every word w * 2^64 mod
+// p, any 64-bit representative): the form the reference's BFieldElement keeps
+// internally.  The byte lookups then need no conversion, the x^7 products
+// reduce by gl_redc, and the MDS, being linear with integer entries, commutes
+// with the form; its round constants are stored in Montgomery form.
+__device__ __forceinline__ void t5_permutation_m(uint64_t s[T5_STATE], const uint32_t* lane_tbl) {
 #pragma unroll 1
     for (int rnd = 0; rnd < T5_ROUNDS; rnd++) {
 #pragma unroll
-        for (int i = 0; i < 4; i++) s[i] = t5_split_lookup(s[i], lane_tbl);
-        t5_pow7_layer(s);
+        for (int i = 0; i < 4; i++) s[i] = t5_split_lookup_m(s[i], lane_tbl);
+        t5_pow7_layer_m(s);
         t5_mds(s, rnd);  // and the round constants
     }
 }
 
-// One round (Tip5::round, src/hash/tip5.cpp:114-118) for the off-path
-// single-round and trace entry points; the hashing kernels use t5_permutation.
-__device__ __forceinline__ void t5_round(uint64_t s[T5_STATE], const uint32_t* lane_tbl, int rnd) {
+// The permutation on a plain state (any representatives in, canonical out).
+__device__ __forceinline__ void t5_permutation(uint64_t s[T5_STATE], const uint32_t* lane_tbl) {
 #pragma unroll
-    for (int i = 0; i < 4; i++) s[i] = t5_split_lookup(s[i], lane_tbl);
-    t5_pow7_layer(s);
-    t5_mds(s, rnd);
+    for (int i = 0; i < T5_STATE; i++) s[i] = gl_to_mont(s[i]);
+    t5_permutation_m(s, lane_tbl);
+#pragma unroll
+    for (int i = 0; i < T5_STATE; i++) s[i] = gl_from_mont(s[i]);
 }
 
-// Tip5::hash_pair / hash_10: rate = left || right, capacity = 1s.
+// One round (Tip5::round, src/hash/tip5.cpp:114-118) on a plain state, for the
+// off-path single-round and trace entry points.
+__device__ __forceinline__ void t5_round(uint64_t s[T5_STATE], const uint32_t* lane_tbl, int rnd) {
+#pragma unroll
+    for (int i = 0; i < T5_STATE; i++) s[i] = gl_to_mont(s[i]);
+#pragma unroll
+    for (int i = 0; i < 4; i++) s[i] = t5_split_lookup_m(s[i], lane_tbl);
+    t5_pow7_layer_m(s);
+    t5_mds(s, rnd);
+#pragma unroll
+    for (int i = 0; i < T5_STATE; i++) s[i] = gl_from_mont(s[i]);
+}
+
+// Tip5::hash_pair / hash_10: rate = left || right, capacity = 1s; plain digests
+// in, canonical digest out.
 __device__ __forceinline__ void t5_hash_pair(const uint64_t l[5], const uint64_t r[5], uint64_t out[5],
                                              const uint32_t* lane_tbl) {
     uint64_t s[T5_STATE];
 #pragma unroll
-    for (int i = 0; i < 5; i++) { s[i] = l[i]; s[5 + i] = r[i]; }
+    for (int i = 0; i < 5; i++) { s[i] = gl_to_mont(l[i]); s[5 + i] = gl_to_mont(r[i]); }
 #pragma unroll
-    for (int i = T5_RATE; i < T5_STATE; i++) s[i] = 1;
-    t5_permutation(s, lane_tbl);
+    for (int i = T5_RATE; i < T5_STATE; i++) s[i] = T5_MONT_ONE;
+    t5_permutation_m(s, lane_tbl);
 #pragma unroll
-    for (int i = 0; i < 5; i++) out[i] = gl_canon(s[i]);
+    for (int i = 0; i < 5; i++) out[i] = gl_from_mont(s[i]);
 }
 
 }  // namespace tvmc
