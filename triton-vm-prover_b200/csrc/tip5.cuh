@@ -51,6 +51,10 @@ constexpr uint64_t t5_to_mont_const(uint64_t x) {
     const uint64_t v = (x & 0xFFFFFFFFull) * 0xFFFFFFFFull, x1 = x >> 32;
     return v >= x1 ? v - x1 : GL_P - (x1 - v);
 }
+// t5_recombine takes the high words of the biased MDS halves as they are,
+// exponent bits included: each is L1 + K (H1 + K) with K = 0x43300000, which
+// adds 2K * 2^32 - K to every result; the round constants carry its negative.
+constexpr uint64_t T5_RECOMBINE_EXCESS = 2ull * 0x43300000ull * 0x100000000ull - 0x43300000ull;
 // The round constants enter in Montgomery form, like the state (t5_permutation_m).
 struct T5RoundBias {
     double lo[T5_ROUNDS * T5_STATE];  // T5_MDS_BIAS + (rc * 2^64 mod p) & (2^32 - 1)
@@ -60,7 +64,9 @@ constexpr T5RoundBias t5_round_bias() {
     const uint64_t rc[T5_ROUNDS * T5_STATE] = {TVMC_T5_ROUND_CONSTANTS};
     T5RoundBias b{};
     for (int i = 0; i < T5_ROUNDS * T5_STATE; i++) {
-        const uint64_t m = t5_to_mont_const(rc[i]);
+        // less the constant that t5_recombine's unmasked high limbs add
+        const uint64_t m0 = t5_to_mont_const(rc[i]);
+        const uint64_t m = m0 >= T5_RECOMBINE_EXCESS ? m0 - T5_RECOMBINE_EXCESS : m0 + (GL_P - T5_RECOMBINE_EXCESS);
         b.lo[i] = T5_MDS_BIAS + (double)(uint32_t)m;
         b.hi[i] = T5_MDS_BIAS + (double)(uint32_t)(m >> 32);
     }
@@ -213,12 +219,15 @@ __device__ __forceinline__ double t5_half_biased(uint32_t v) {
 // (L1, H1 < 2^20), lo + hi*2^32 = L0 + (L1 + H0)*2^32 + H1*2^64, and
 // 2^64 = 2^32 - 1 (mod p) turns it into L0 - H1 + (H0 + L1 + H1)*2^32.  The
 // carry c of the high sum and the borrows of the subtraction net to c in
-// {-1, 0, 1}, folded back as c*(2^32 - 1): for c = 1 the high limb is below
-// 2^21, for c = -1 it is 2^32 - 1, so the fold cannot wrap.  The low limbs of the
-// doubles are L0 and H0 as they are; only the high limbs need masking.
+// {-1, 0, 1}, folded back as c*(2^32 - 1): for c = 1 the high limb is at most
+// 2^32 - 2, for c = -1 it is 2^32 - 1, so the fold cannot wrap.  The low limbs of
+// the doubles are L0 and H0 as they are; the high limbs enter unmasked, as
+// L1 + K and H1 + K (K = 0x43300000, the exponent bits; 2K + L1 + H1 < 2^32),
+// and the constant this adds is taken out of the round constants
+// (T5_RECOMBINE_EXCESS).
 __device__ __forceinline__ uint64_t t5_recombine(double dlo, double dhi) {
-    const uint32_t l0 = (uint32_t)__double2loint(dlo), l1 = (uint32_t)__double2hiint(dlo) & 0xFFFFFu;
-    const uint32_t h0 = (uint32_t)__double2loint(dhi), h1 = (uint32_t)__double2hiint(dhi) & 0xFFFFFu;
+    const uint32_t l0 = (uint32_t)__double2loint(dlo), l1 = (uint32_t)__double2hiint(dlo);
+    const uint32_t h0 = (uint32_t)__double2loint(dhi), h1 = (uint32_t)__double2hiint(dhi);
     uint32_t x0, x1;
     asm("{\n\t"
         ".reg .u32 a, c, e0, e1;\n\t"
