@@ -101,13 +101,14 @@ __device__ __forceinline__ void t5_sbox_init(uint32_t* tbl) {
 }
 
 // Byte-wise S-box of a 32-bit word through the lane's private table column:
-// each lookup returns its byte in bits 0-7, so the assembly is three byte
-// permutes with constant selectors.
+// each index byte is extracted by one byte permute (selector 0x444k: byte k,
+// zero-extended), each lookup returns its byte in bits 0-7, so the assembly is
+// three byte permutes with constant selectors.
 __device__ __forceinline__ uint32_t t5_lookup32(uint32_t m, const uint32_t* lane_tbl) {
-    const uint32_t w0 = lane_tbl[(m & 255) << 5];
-    const uint32_t w1 = lane_tbl[((m >> 8) & 255) << 5];
-    const uint32_t w2 = lane_tbl[((m >> 16) & 255) << 5];
-    const uint32_t w3 = lane_tbl[(m >> 24) << 5];
+    const uint32_t w0 = lane_tbl[__byte_perm(m, 0, 0x4440) << 5];
+    const uint32_t w1 = lane_tbl[__byte_perm(m, 0, 0x4441) << 5];
+    const uint32_t w2 = lane_tbl[__byte_perm(m, 0, 0x4442) << 5];
+    const uint32_t w3 = lane_tbl[__byte_perm(m, 0, 0x4443) << 5];
     return __byte_perm(__byte_perm(w0, w1, 0x0040), __byte_perm(w2, w3, 0x0040), 0x5410);
 }
 
