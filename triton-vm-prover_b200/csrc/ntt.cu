@@ -632,13 +632,14 @@ __global__ void __launch_bounds__(128, MINB) k_lde_mid_sym(const uint64_t* Y, ui
 
 // K2, table-sharing form of k_lde_mid_sym: the inter-pass twiddles
 // w_N^(k2*q) are the same for all E cosets, so the CTA forms them once into
-// shared memory (twq, T*n1 words) and every coset reads them there; the coset
-// scale N^-1 s_c^i, i = i0 + n2*R*k1 with i0 = k2 + n2*ln, is split into a
-// per-thread factor A_c = N^-1 s_c^i0 (one per coset) and a per-CTA table
-// sb[c][k1] = s_c^(n2*R*k1); the sub-transform twiddles stay in shared memory
-// as in k_lde_mid_sym.  Per element and coset this replaces four global table
-// loads and one general product by two shared-memory loads.  At n1 = 2^10 the
-// CTA holds 74 KB of shared memory, so three CTAs still fit on an SM.
+// shared memory (twq, T*n1 words) and every coset reads them there.  The coset
+// scale N^-1 s_c^i, i = k2 + n2*ln + n2*R*k1, costs one product per element:
+// s_c^(n2*ln) is constant over round 1's input index k1, so it rides on that
+// round's output twiddle, whose per-coset table twf[ln][k] = w_n1^(ln*k)
+// s_c^(n2*ln) the CTA refills before each coset; the rest comes from a
+// per-coset table sbt[t][k1] = N^-1 s_c^(k2 + n2*R*k1).  All factors are in
+// Montgomery form.  At n1 = 2^10 the CTA holds 74 KB of shared memory, so three
+// CTAs still fit on an SM.
 template <int L1, int MINB, bool RAND>
 __global__ void __launch_bounds__(128, MINB) k_lde_mid_sym2(const uint64_t* Y, uint64_t yld, uint64_t* Z, int l2,
                                                             int le, const uint64_t* tw12_f, const uint64_t* wlo,
@@ -650,23 +651,34 @@ __global__ void __launch_bounds__(128, MINB) k_lde_mid_sym2(const uint64_t* Y, u
     constexpr int B = PL::b1, R = 1 << B;
     constexpr int lT = 7 - B, T = 1 << lT;  // T * R = 128 threads
     constexpr int n1 = 1 << L1;
+    constexpr int RP = R + 1;  // padded table rows: the warp's lines (rows) fall in distinct banks
     extern __shared__ uint64_t sm[];
-    uint64_t* twf = sm;                        // w_n1^m, m < n1 (forward root only)
-    uint64_t* s = twf + n1;                    // transposes
+    uint64_t* twf = sm;                        // [ln*RP + k]: round-1 output twiddle of line ln, output k
+    uint64_t* s = twf + R * RP;                // transposes
     uint64_t* twq = s + spad_words(n1, lT);    // w_N^((k20 + tt) * q) at [tt + T*q]
-    uint64_t* sb = twq + (T << L1);            // s_c^(n2*R*k1) at [c*R + k1]
-    load_tw<L1, true>(twf, tw12_f);
+    uint64_t* sbt = twq + (T << L1);           // [t*RP + k1]: round-1 input scale of row t, element k1
     const int E = 1 << le;
     const uint64_t col = blockIdx.y;
     const uint32_t k20 = blockIdx.x << lT;
     const uint64_t N = 1ull << (L1 + l2);
+    // twf holds w_n1^(ln*k) for the inverse and w_n1^(ln*k) * s_c^(n2*ln) for
+    // coset c (Montgomery form): each thread fills KPT consecutive k of line bl,
+    // forming the line factor bm once.
+    constexpr int KPT = R * R >= 128 ? R * R / 128 : 1;
+    const int bl = threadIdx.x / (R / KPT), bk = (threadIdx.x % (R / KPT)) * KPT;
+    auto fill_twf = [&](uint64_t bm) {
+        if (bl < R) {
+#pragma unroll
+            for (int j = 0; j < KPT; j++) {
+                const int k = bk + j;
+                const uint64_t w = __ldg(tw12_f + (((bl * k) & (n1 - 1)) << (12 - L1)));
+                twf[bl * RP + k] = gl_mont_mul(gl_to_mont(w), bm);
+            }
+        }
+    };
+    fill_twf(0xFFFFFFFFull);  // 1 in Montgomery form
     for (int idx = threadIdx.x; idx < (T << L1); idx += blockDim.x)
         twq[idx] = gl_to_mont(tw2(wlo, whi, (k20 + (idx & (T - 1))) * (uint32_t)(idx >> lT)));
-    for (int idx = threadIdx.x; idx < (E << B); idx += blockDim.x) {
-        const int c = idx >> B, k1 = idx & (R - 1);
-        // tw2 on the scale tables carries N^-1; multiplying by N cancels it
-        sb[idx] = gl_to_mont(gl_mul(tw2(sc_lo + 4096 * c, sc_hi + hi_len * c, ((uint32_t)k1 << (B + l2))), N));
-    }
     __syncthreads();
     const uint64_t* src = Y + col * yld + ((uint64_t)k20 << L1);
     const int t = threadIdx.x & (T - 1), ln = threadIdx.x >> lT;
@@ -675,7 +687,21 @@ __global__ void __launch_bounds__(128, MINB) k_lde_mid_sym2(const uint64_t* Y, u
 #pragma unroll 1
     for (int pass = 0; pass <= E; pass++) {  // 0: inverse; c + 1: forward, coset c
         const int c = pass ? pass - 1 : 0;
-        const uint64_t a_c = gl_to_mont(tw2(sc_lo + 4096 * c, sc_hi + hi_len * c, i0));
+        if (pass) {
+            // the coset scale N^-1 s_c^i, i = k2 + n2*ln + n2*R*k1, k2 = k20 + t:
+            // s_c^(n2*ln) is constant over round 1's input index k1, so it joins
+            // that round's output twiddle (twf); the rest is one table entry per
+            // (row t, element k1) (sbt).  tw2 on the scale tables carries N^-1.
+            const uint64_t* lo = sc_lo + 4096 * c;
+            const uint64_t* hi = sc_hi + hi_len * c;
+            fill_twf(bl < R ? gl_to_mont(gl_mul(tw2(lo, hi, (uint32_t)bl << l2), N)) : 0);
+            for (int idx = threadIdx.x; idx < T * R; idx += blockDim.x) {
+                const int tt = idx >> B, k1 = idx & (R - 1);
+                sbt[tt * RP + k1] = gl_to_mont(
+                    gl_mul(gl_mul(tw2(lo, hi, k20 + tt), tw2(lo, hi, (uint32_t)k1 << (B + l2))), N));
+            }
+            __syncthreads();
+        }
 #pragma unroll 1
         for (int half = 0; half < 2; half++) {
             uint64_t v[R];
@@ -683,7 +709,7 @@ __global__ void __launch_bounds__(128, MINB) k_lde_mid_sym2(const uint64_t* Y, u
                 if (pass == 0) {  // inverse round 1: elements -(ln + R*j) of row t
 #pragma unroll
                     for (int j = 0; j < R; j++) v[j] = src[((uint64_t)t << L1) + (-(ln + (j << B)) & (n1 - 1))];
-                } else {  // forward round 1: c[ln + R*k1] * A_c * sb[c][k1]
+                } else {  // forward round 1: c[ln + R*k1] * N^-1 s_c^(k2 + n2*R*k1)
 #pragma unroll
                     for (int k1 = 0; k1 < R; k1++) {
                         uint64_t x = cf[k1];
@@ -691,7 +717,7 @@ __global__ void __launch_bounds__(128, MINB) k_lde_mid_sym2(const uint64_t* Y, u
                             const uint32_t i = i0 + ((uint32_t)k1 << (B + l2));
                             if (i < (uint32_t)rm) x = gl_add_pc(x, add[(col * E + c) * rm + i]);
                         }
-                        v[k1] = gl_mont_mul(gl_mont_mul(x, sb[c * R + k1]), a_c);
+                        v[k1] = gl_mont_mul(x, sbt[t * RP + k1]);
                     }
                 }
             } else {  // round 2 of either: slots x + R*ln
@@ -699,11 +725,11 @@ __global__ void __launch_bounds__(128, MINB) k_lde_mid_sym2(const uint64_t* Y, u
                 for (int x = 0; x < R; x++) v[x] = s[spos2<B>(x, ln, lT) + t];
             }
             reg_dft<B>(v);
-            if (half == 0) {  // twiddle w_n1^(ln*k), slot ln + R*k
+            if (half == 0) {  // twiddle twf[ln][k], slot ln + R*k
 #pragma unroll
                 for (int k = 0; k < R; k++) {
                     uint64_t x = v[brevc<B>(k)];
-                    if (ln * k) x = gl_mont_mul(x, twf[ln * k]);
+                    if (pass || ln * k) x = gl_mont_mul(x, twf[ln * RP + k]);
                     s[spos2<B>(ln, k, lT) + t] = x;
                 }
             } else if (pass == 0) {
@@ -982,8 +1008,9 @@ cudaError_t launch_lde(const LdePlan& pl, const uint64_t* trace, uint64_t tld, u
             if constexpr (Plan<L1>::NR == 2 && Plan<L1>::b1 == Plan<L1>::b2) {
                 constexpr int lTr = 7 - Plan<L1>::b2;
                 if (tuning_lde_mid_variant() == 2) {
-                    const size_t sm2 = words_bytes(((size_t)1 << L1) + spad_words(1 << L1, lTr) +
-                                                   ((size_t)1 << (lTr + L1)) + ((size_t)1 << (le + Plan<L1>::b2)));
+                    constexpr size_t R2 = (size_t)1 << Plan<L1>::b2;
+                    const size_t sm2 = words_bytes(R2 * (R2 + 1) + spad_words(1 << L1, lTr) +
+                                                   ((size_t)1 << (lTr + L1)) + ((size_t)1 << lTr) * (R2 + 1));
                     auto kern = rm ? k_lde_mid_sym2<L1, 2, true>
                                    : (tuning_lde_mid_ctas() == 3 ? k_lde_mid_sym2<L1, 3, false>
                                                                  : k_lde_mid_sym2<L1, 2, false>);
