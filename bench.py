@@ -548,10 +548,10 @@ def run_ours(args):
                    "cost_model": f"Tip5 {OPS_PER_PERM} int32 ops per permutation; NTT {OPS_PER_NTT_MUL} per "
                                  "butterfly or scale; bytes 8NW + 32NW + 40*4N + 40*(4N-1) per table"}
     # DRAM bytes per k_hash_rows launch: one ncu capture of the 2^18-row x 379-column
-    # main-table launch (795.3 MB read + 17.4 MB written), scaled by rows
+    # main-table launch (795.6 MB read + 16.0 MB written), scaled by rows
     traffic, traffic_src = None, None
     if W_MAIN == 379:
-        traffic = (795.35e6 + 17.45e6) * L / (1 << 18)
+        traffic = (795.59e6 + 16.05e6) * L / (1 << 18)
         traffic_src = "ncu dram__bytes_read+write of a 2^18x379 launch, scaled by LDE rows (main table)"
 
     # e2e: pinned host traces through the public C ABI, roots read back
