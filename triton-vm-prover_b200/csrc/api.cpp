@@ -284,8 +284,9 @@ struct ScratchSlot {
     // (the next upload into it waits for this, not for the whole stream)
     cudaEvent_t last_use = nullptr;
 };
-// kind: 0 = LDE/NTT intermediates, 1 and 2 = the two upload staging buffers,
-// 3 = the LDE of commits that discard it after hashing.
+// kind: 0 = LDE/NTT intermediates, 1 and 2 = the first two upload staging
+// buffers (UPLOAD_STAGES in all: stage_kind), 3 = the LDE of commits that
+// discard it after hashing, 4 = the multi-table staging buffer.
 std::map<std::tuple<int, cudaStream_t, int>, ScratchSlot> g_scratch;  // guarded by g_mu
 
 // *grown (optional) is set when the buffer was (re)allocated by this call, i.e.
@@ -386,9 +387,14 @@ int copy_stream(cudaStream_t compute, cudaStream_t* out) {
     return TVMC_OK;
 }
 
-// Host column-major trace -> device LDE.  Column chunks are staged through two
-// device buffers: the copy stream uploads chunk k+1 while `st` runs the LDE of
-// chunk k.  Returns after enqueueing; `st` is ordered after every copy.
+// Host column-major trace -> device LDE.  Column chunks of about 256 MB are
+// staged through UPLOAD_STAGES device buffers per stream: the copy stream uploads
+// ahead while `st` runs the LDE of an earlier chunk, and a commit's first
+// UPLOAD_STAGES chunks wait only for the previous commit's LDE kernels that read
+// those buffers, so they upload during that commit's row hash.  Returns after
+// enqueueing; `st` is ordered after every copy.
+constexpr int UPLOAD_STAGES = 4;
+constexpr int stage_kind(int b) { return b < 2 ? 1 + b : 16 + b; }
 int upload_lde_pipelined(const LdePlan& pl, const uint64_t* h_trace, size_t n, size_t width, uint64_t* d_out,
                          size_t L, cudaStream_t st, const RandAdd& ra = RandAdd{}) {
     cudaStream_t cs = nullptr;
@@ -400,24 +406,25 @@ int upload_lde_pipelined(const LdePlan& pl, const uint64_t* h_trace, size_t n, s
     chunk = std::min(chunk, stage_cols);
     const size_t nchunks = (width + chunk - 1) / chunk;
     std::lock_guard<std::mutex> turn(upload_mutex(st));
-    uint64_t *scratch = nullptr, *stage[2] = {nullptr, nullptr};
-    cudaEvent_t ready[2] = {nullptr, nullptr}, freed[2] = {nullptr, nullptr}, prev[2] = {nullptr, nullptr};
-    bool used[2] = {false, false};
+    const int nst = (int)std::min<size_t>(UPLOAD_STAGES, nchunks);
+    uint64_t *scratch = nullptr, *stage[UPLOAD_STAGES] = {};
+    cudaEvent_t ready[UPLOAD_STAGES] = {}, freed[UPLOAD_STAGES] = {}, prev[UPLOAD_STAGES] = {};
+    bool used[UPLOAD_STAGES] = {};
     if ((rc = stream_scratch(st, lde_scratch_words(pl.logn, pl.log_exp, chunk), &scratch))) return rc;
     cudaError_t e = cudaSuccess;
-    for (int b = 0; b < 2 && e == cudaSuccess; b++) {
+    for (int b = 0; b < nst && e == cudaSuccess; b++) {
         bool grown = false;
-        if (stream_scratch(st, chunk * n, &stage[b], 1 + b, &grown)) e = cudaErrorMemoryAllocation;
+        if (stream_scratch(st, chunk * n, &stage[b], stage_kind(b), &grown)) e = cudaErrorMemoryAllocation;
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ready[b], cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&freed[b], cudaEventDisableTiming);
         // The first copy into stage[b] waits for the last kernel that read it (the
         // previous commit's on this stream), so it can overlap that commit's row
         // hash; a freshly allocated buffer is ordered on st instead.
-        if (e == cudaSuccess && !grown) prev[b] = take_slot_event(st, 1 + b);
+        if (e == cudaSuccess && !grown) prev[b] = take_slot_event(st, stage_kind(b));
         if (e == cudaSuccess && !prev[b]) e = cudaEventRecord(freed[b], st);
     }
     for (size_t k = 0; k < nchunks && e == cudaSuccess; k++) {
-        const int b = (int)(k & 1);
+        const int b = (int)(k % (size_t)nst);
         const size_t c0 = k * chunk, nc = std::min(chunk, width - c0);
         e = cudaStreamWaitEvent(cs, (!used[b] && prev[b]) ? prev[b] : freed[b], 0);
         used[b] = true;
@@ -428,14 +435,14 @@ int upload_lde_pipelined(const LdePlan& pl, const uint64_t* h_trace, size_t n, s
         if (e == cudaSuccess) e = launch_lde(pl, stage[b], n, d_out + c0 * L, L, nc, scratch, st, ra.cols(c0), ra.rm);
         if (e == cudaSuccess) e = cudaEventRecord(freed[b], st);
     }
-    for (int b = 0; b < 2; b++) {
+    for (int b = 0; b < nst; b++) {
         if (ready[b]) cudaEventDestroy(ready[b]);  // destruction is deferred until the event completes
         if (e == cudaSuccess && used[b]) {
-            give_slot_event(st, 1 + b, freed[b]);  // recorded after the last kernel reading stage[b]
+            give_slot_event(st, stage_kind(b), freed[b]);  // recorded after the last kernel reading stage[b]
             if (prev[b]) cudaEventDestroy(prev[b]);
         } else {
             if (freed[b]) cudaEventDestroy(freed[b]);
-            if (prev[b]) give_slot_event(st, 1 + b, prev[b]);  // still the guard for that buffer
+            if (prev[b]) give_slot_event(st, stage_kind(b), prev[b]);  // still the guard for that buffer
         }
     }
     if (e != cudaSuccess) return cuda_fail(e, "pipelined upload/LDE");
