@@ -74,7 +74,12 @@ void footprint(Request* r, bool keep_lde, size_t scratch_budget) {
     const size_t scratch = N > 2048 ? std::min(scratch_budget, N * (1 + r->expansion) * 8 * std::max<size_t>(W, 1)) : 0;
     size_t upload = 0;
     if (frugal) upload = (dev ? 0 : NW) + (rm ? NW : 0) + 6 * L * 8;
-    else if (!dev && !rm) upload = 2 * std::min<size_t>(NW, size_t(256) << 20);
+    else if (!dev && !rm) {
+        // host uploads stage column chunks of about 256 MB through up to four
+        // buffers per stream (fewer when the table has fewer chunks)
+        const size_t stage = std::min<size_t>(NW, size_t(256) << 20);
+        upload = std::min<size_t>(4, (NW + stage - 1) / stage) * stage;
+    }
     else upload = (dev ? 0 : NW) + (rm ? NW : 0);
     // randomized LDE: randomizer upload and the per-coset addends
     const size_t rrows = r->R < N ? r->R : N;
